@@ -1,0 +1,735 @@
+/*
+ * mmff_oracle.c -- FP64 CPU restatement of the MMFF multi-system relaxation
+ * hot path (TEST INFRASTRUCTURE: the checker, never the product).
+ *
+ * Each function names the reference function (file:line inside the FireCore
+ * tree) whose arithmetic it restates.  Operation order follows the reference
+ * so that FP64 results agree to rounding with the compiled reference harness
+ * (oracle/ref_harness.cpp) on the golden fixtures.
+ *
+ * Extension beyond the reference (documented, off by default): an optional
+ * smooth non-bonded cutoff (P->Rcut > 0).  With Rcut <= 0 the pair sum is the
+ * reference's all-pairs x all-images sum.
+ */
+#include "mmff_oracle.h"
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define COULOMB_CONST 14.3996448915   /* cpp/common_resources/cl/relax_multi.cl:79, constants.h */
+
+typedef struct { double x, y, z; } v3;
+
+static inline v3   v3make(double x, double y, double z) { v3 r = {x, y, z}; return r; }
+static inline v3   vadd(v3 a, v3 b) { return v3make(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline v3   vsub(v3 a, v3 b) { return v3make(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline v3   vmul(v3 a, double f) { return v3make(a.x * f, a.y * f, a.z * f); }
+static inline double vdot(v3 a, v3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+/* a += b*f  (Vec3::add_mul) */
+static inline v3   vaddmul(v3 a, v3 b, double f) { return v3make(a.x + b.x * f, a.y + b.y * f, a.z + b.z * f); }
+/* A*fa + B*fb  (Vec3::set_lincomb) */
+static inline v3   vlin(double fa, v3 A, double fb, v3 B) { return v3make(A.x * fa + B.x * fb, A.y * fa + B.y * fb, A.z * fa + B.z * fb); }
+
+static inline v3 ld3(const double* p) { return v3make(p[0], p[1], p[2]); }
+static inline void st3(double* p, v3 v) { p[0] = v.x; p[1] = v.y; p[2] = v.z; }
+
+/* ---------------- scalar force kernels (cpp/common/math/Forces.h) ---------------- */
+
+/* Forces.h:137 evalBond */
+static inline double evalBond(v3 h, double dl, double k, v3* f) {
+    double fr = dl * k;
+    *f = vmul(h, fr);
+    return fr * dl * 0.5;
+}
+
+/* Forces.h:190 evalAngleCosHalf (Vec2::udiv_cmplx, math/Vec2.h:130) */
+static inline double evalAngleCosHalf(v3 h1, v3 h2, double ir1, double ir2,
+                                      double cs0x, double cs0y, double k, v3* f1, v3* f2) {
+    v3 h = vadd(h1, h2);
+    double c2 = vdot(h, h) * 0.25;
+    double s2 = 1 - c2 + 1e-14;
+    double c = sqrt(c2);
+    double s = sqrt(s2);
+    double csx = cs0x * c + cs0y * s;
+    double csy = cs0y * c - cs0x * s;
+    double E = k * (1 - csx);
+    double fr = -k * (csy);
+    c2 *= -2;
+    fr /= 4 * c * s;
+    double fr1 = fr * ir1;
+    double fr2 = fr * ir2;
+    *f1 = vlin(fr1, h, fr1 * c2, h1);
+    *f2 = vlin(fr2, h, fr2 * c2, h2);
+    return E;
+}
+
+/* Forces.h:217 evalAngleCos */
+static inline double evalAngleCos(v3 h1, v3 h2, double ir1, double ir2, double K, double c0, v3* f1, v3* f2) {
+    double c = vdot(h1, h2);
+    v3 a = vaddmul(h2, h1, -c);
+    v3 b = vaddmul(h1, h2, -c);
+    double c_ = c - c0;
+    double E = K * c_ * c_;
+    double fang = -K * c_ * 2;
+    *f1 = vmul(a, fang * ir1);
+    *f2 = vmul(b, fang * ir2);
+    return E;
+}
+
+/* Forces.h:230 evalPiAling */
+static inline double evalPiAling(v3 h1, v3 h2, double K, v3* f1, v3* f2) {
+    double c = vdot(h1, h2);
+    v3 a = vaddmul(h2, h1, -c);
+    v3 b = vaddmul(h1, h2, -c);
+    int sign = c < 0; if (sign) c = -c;
+    double E = K * (1 - c);
+    double fang = K;
+    if (sign) fang = -fang;
+    *f1 = vmul(a, fang);
+    *f2 = vmul(b, fang);
+    return E;
+}
+
+/* Forces.h:341 getLJQH (undamped Coulomb + H-bond correction); REQ already mixed */
+static inline double getLJQH(v3 dp, const double* REQ, v3* f) {
+    const double r2 = vdot(dp, dp);
+    const double ir2 = 1 / r2;
+    double E = COULOMB_CONST * REQ[2] * sqrt(ir2);
+    double F = E * ir2;
+    const double u2 = REQ[0] * REQ[0] * ir2;
+    const double u6 = u2 * u2 * u2;
+    const double vdW = u6 * REQ[1];
+    const double H = u6 * u6 * ((REQ[3] < 0) ? REQ[3] * REQ[1] : 0.0);
+    E += (u6 - 2.) * vdW + H;
+    F += ((u6 - 1.) * vdW + H) * ir2 * 12;
+    *f = vmul(dp, -F);
+    return E;
+}
+
+/* Forces.h:270 _mixREQ */
+static inline void mixREQ(const double* A, const double* B, double* o) {
+    o[0] = A[0] + B[0]; o[1] = A[1] * B[1]; o[2] = A[2] * B[2]; o[3] = A[3] * B[3];
+}
+
+/* clampForce (Forces.h) : scale f so |f|^2 <= Fmax2 */
+static inline v3 clampForce(v3 f, double Fmax2) {
+    double f2 = vdot(f, f);
+    if (f2 > Fmax2) { f = vmul(f, sqrt(Fmax2 / f2)); }
+    return f;
+}
+
+/* NBFF.h:42 makePBCshifts_ ordering: iz outer, iy, ix inner */
+static inline v3 pbc_shift(const double* lv, const int* np, int ipbc) {
+    int nx = 2 * np[0] + 1, ny = 2 * np[1] + 1;
+    int ix = ipbc % nx - np[0];
+    int iy = (ipbc / nx) % ny - np[1];
+    int iz = ipbc / (nx * ny) - np[2];
+    v3 a = ld3(lv), b = ld3(lv + 3), c = ld3(lv + 6);
+    return vadd(vadd(vmul(a, ix), vmul(b, iy)), vmul(c, iz));
+}
+
+typedef struct {
+    int natoms, nnode, nvecs;
+    const double* pos;       /* [nvecs*3] */
+    const int* neighs; const int* neighCell; const int* bkneighs;
+    const double* REQs; const double* apars; const double* bLs; const double* bKs;
+    const double* Ksp; const double* Kpp; const double* lvec;
+    double* fneigh;          /* [nnode*4*3] */
+    double* fneighpi;        /* [nnode*4*3] */
+    double* force;           /* [nvecs*3] */
+    v3* shifts;              /* [npbc] */
+    int npbc;
+} sysview;
+
+/* MMFFsp3_loc.h:250-575 eval_atom (non-templated path; no collision damping,
+ * bEachAngle=false, bAngleCosHalf=true) */
+static double eval_atom(const sysview* S, const ORC_params* P, int ia) {
+    const int flags = P->flags;
+    double E = 0;
+    const double Fmax2 = P->FmaxNonBonded * P->FmaxNonBonded;
+    const v3 pa = ld3(S->pos + 3 * ia);
+    const v3 hpi = ld3(S->pos + 3 * (S->natoms + ia));
+    v3 fa = v3make(0, 0, 0), fpi = v3make(0, 0, 0);
+    const int* ings = S->neighs + ia * 4;
+    const int* ingC = S->neighCell + ia * 4;
+    const double* bK = S->bKs + ia * 4;
+    const double* bL = S->bLs + ia * 4;
+    const double* Kspi = S->Ksp + ia * 4;
+    const double* Kppi = S->Kpp + ia * 4;
+    double* fbs = S->fneigh + ia * 12;
+    double* fps = S->fneighpi + ia * 12;
+    const double* apar = S->apars + ia * 4;
+    const double piC0 = apar[3];
+    v3 hsf[4]; double hse[4];
+    v3 f1, f2;
+    v3 fb[4], fp[4];
+    for (int i = 0; i < 4; i++) { fb[i] = v3make(0, 0, 0); fp[i] = v3make(0, 0, 0); }
+
+    for (int i = 0; i < 4; i++) {
+        int ing = ings[i];
+        if (ing < 0) break;
+        v3 h = vsub(ld3(S->pos + 3 * ing), pa);
+        if (flags & ORC_PBC) { h = vadd(h, S->shifts[ingC[i]]); }
+        /* Vec3::normalize (math/Vec3.h:149) */
+        double l = sqrt(h.x * h.x + h.y * h.y + h.z * h.z);
+        double il = 1.0 / l;
+        h = vmul(h, il);
+        double he = 1 / l;
+        hsf[i] = h; hse[i] = he;
+        if (ia < ing) {
+            if (flags & ORC_BONDS) {
+                E += evalBond(h, l - bL[i], bK[i], &f1);
+                if (flags & ORC_SUB_BOND_NB) {
+                    double REQij[4]; mixREQ(S->REQs + 4 * ia, S->REQs + 4 * ing, REQij);
+                    v3 dp = vmul(h, l);
+                    v3 fij;
+                    E -= getLJQH(dp, REQij, &fij);
+                    if (flags & ORC_CLAMP_NB) fij = clampForce(fij, Fmax2);
+                    f1 = vsub(f1, fij);
+                }
+                fb[i] = vsub(fb[i], f1); fa = vadd(fa, f1);
+            }
+            double kpp = Kppi[i];
+            if ((flags & ORC_PIPI) && (ing < S->nnode) && (kpp > 1e-6)) {
+                E += evalPiAling(hpi, ld3(S->pos + 3 * (S->natoms + ing)), kpp, &f1, &f2);
+                fpi = vadd(fpi, f1); fp[i] = vadd(fp[i], f2);
+            }
+        }
+        double ksp = Kspi[i];
+        if ((flags & ORC_PISIGMA) && (ksp > 1e-6)) {
+            E += evalAngleCos(hpi, h, 1., he, ksp, piC0, &f1, &f2);
+            fpi = vadd(fpi, f1); fa = vsub(fa, f2); fb[i] = vadd(fb[i], f2);
+        }
+    }
+    if (flags & ORC_ANGLES) {
+        const double ssK = apar[2];
+        const double cs0x = apar[0], cs0y = apar[1];
+        for (int i = 0; i < 3; i++) {
+            int ing = ings[i];
+            if (ing < 0) break;
+            for (int j = i + 1; j < 4; j++) {
+                int jng = ings[j];
+                if (jng < 0) break;
+                E += evalAngleCosHalf(hsf[i], hsf[j], hse[i], hse[j], cs0x, cs0y, ssK, &f1, &f2);
+                fa = vsub(fa, vadd(f1, f2));
+                if (flags & ORC_SUB_ANGLE_NB) {
+                    double REQij[4]; mixREQ(S->REQs + 4 * ing, S->REQs + 4 * jng, REQij);
+                    v3 dp = vlin(1. / hse[j], hsf[j], -1. / hse[i], hsf[i]);
+                    v3 fij;
+                    E -= getLJQH(dp, REQij, &fij);
+                    if (flags & ORC_CLAMP_NB) fij = clampForce(fij, Fmax2);
+                    f1 = vsub(f1, fij);
+                    f2 = vadd(f2, fij);
+                }
+                fb[i] = vadd(fb[i], f1);
+                fb[j] = vadd(fb[j], f2);
+            }
+        }
+    }
+    for (int i = 0; i < 4; i++) { st3(fbs + 3 * i, fb[i]); st3(fps + 3 * i, fp[i]); }
+    st3(S->force + 3 * ia, fa);
+    st3(S->force + 3 * (S->natoms + ia), fpi);
+    return E;
+}
+
+/* Smooth cutoff switch on r^2 (extension; not in the reference). */
+static inline double switch_r2(double r2, double Ron2, double inv_w, double* dSdr2) {
+    double t = (r2 - Ron2) * inv_w;
+    if (t <= 0) { *dSdr2 = 0; return 1.0; }
+    if (t >= 1) { *dSdr2 = 0; return 0.0; }
+    *dSdr2 = -6.0 * t * (1.0 - t) * inv_w;
+    return 1.0 - t * t * (3.0 - 2.0 * t);
+}
+
+/* NBFF.h:575-618 evalLJQs_ng4_PBC_atom_omp (returns 0.5*E; adds force) */
+static double eval_nb_atom(const sysview* S, const ORC_params* P, int ia) {
+    const v3 pi = ld3(S->pos + 3 * ia);
+    const double* REQi = S->REQs + 4 * ia;
+    const int* ng = S->neighs + 4 * ia;
+    const int* ngC = S->neighCell + 4 * ia;
+    const int usePBC = (P->flags & ORC_PBC) != 0;
+    const int npbc = usePBC ? S->npbc : 1;
+    const int cut = P->Rcut > 0;
+    const double Rc2 = P->Rcut * P->Rcut;
+    const double Ron2 = P->Ron * P->Ron;
+    const double inv_w = cut ? 1.0 / (Rc2 - Ron2) : 0.0;
+    double E = 0, fx = 0, fy = 0, fz = 0;
+    for (int j = 0; j < S->natoms; j++) {
+        if (ia == j) continue;
+        double REQij[4]; mixREQ(REQi, S->REQs + 4 * j, REQij);
+        const v3 dp = vsub(ld3(S->pos + 3 * j), pi);
+        const int bBonded = (j == ng[0]) || (j == ng[1]) || (j == ng[2]) || (j == ng[3]);
+        for (int ipbc = 0; ipbc < npbc; ipbc++) {
+            const v3 dpc = usePBC ? vadd(dp, S->shifts[ipbc]) : dp;
+            if (bBonded) {
+                if (usePBC) {
+                    if (((j == ng[0]) && (ipbc == ngC[0])) || ((j == ng[1]) && (ipbc == ngC[1])) ||
+                        ((j == ng[2]) && (ipbc == ngC[2])) || ((j == ng[3]) && (ipbc == ngC[3]))) continue;
+                } else {
+                    continue;  /* NBFF::evalLJQs_ng4_atom_omp skips bonded j entirely */
+                }
+            }
+            v3 fij;
+            double eij;
+            if (cut) {
+                double r2 = vdot(dpc, dpc);
+                if (r2 >= Rc2) continue;
+                eij = getLJQH(dpc, REQij, &fij);
+                double dS; double Sw = switch_r2(r2, Ron2, inv_w, &dS);
+                fij = vaddmul(vmul(fij, Sw), dpc, 2.0 * eij * dS);
+                eij *= Sw;
+            } else {
+                eij = getLJQH(dpc, REQij, &fij);
+            }
+            E += eij;
+            fx += fij.x; fy += fij.y; fz += fij.z;
+        }
+    }
+    double* f = S->force + 3 * ia;
+    f[0] += fx; f[1] += fy; f[2] += fz;
+    return 0.5 * E;
+}
+
+/* ---------------- B-spline GridFF (cpp/common/math/Bspline.h) ---------------- */
+
+/* Bspline.h:254 basis, :267 dbasis */
+static inline void bs_basis(double u, double* b) {
+    const double inv6 = 1. / 6.;
+    const double u2 = u * u;
+    const double t = 1 - u;
+    b[0] = inv6 * t * t * t;
+    b[1] = inv6 * (3 * u2 * (u - 2) + 4);
+    b[2] = inv6 * (3 * u * (1 + u - u2) + 1);
+    b[3] = inv6 * u2 * u;
+}
+static inline void bs_dbasis(double u, double* d) {
+    const double u2 = u * u;
+    const double t = 1 - u;
+    d[0] = -0.5 * t * t;
+    d[1] = 0.5 * (3 * u2 - 4 * u);
+    d[2] = 0.5 * (-3 * u2 + 2 * u + 1);
+    d[3] = 0.5 * u2;
+}
+
+static inline int modulo_i(int i, int m) { int r = i % m; if (r < 0) r += m; return r; }
+
+/* Bspline.h:36 make_inds_pbc + :43 choose_inds_pbc */
+static inline void choose_inds_pbc(int i, int n, int* q) {
+    if (i >= (n - 3)) {
+        int ii = i + 4 - n;
+        /* iqs[ii] = {0, 1, 2, 3} with the last ii entries wrapped by -n */
+        for (int k = 0; k < 4; k++) q[k] = (k >= 4 - ii) ? k - n : k;
+        return;
+    }
+    q[0] = 0; q[1] = 1; q[2] = 2; q[3] = 3;
+}
+
+/* Bspline.h:742-809 fe3d_pbc_comb3 with fe2d_comb3 (:527) and fe1Dcomb3 (:519);
+ * GridFF.h:355-402 getForce_Bspline (orthorhombic grid, inv_dg2 = -1/step). */
+static void grid_fe(const double* C, const int* gn, const double* pos0, const double* step,
+                    v3 p, const double* PLQ, double* fe) {
+    /* GridFF uses diCell.dot_to(p - pos0) with diCell diagonal = 1/step */
+    const double ux = (p.x - pos0[0]) * (1.0 / step[0]);
+    const double uy = (p.y - pos0[1]) * (1.0 / step[1]);
+    const double uz = (p.z - pos0[2]) * (1.0 / step[2]);
+    const int nx = gn[0], ny = gn[1], nz = gn[2];
+    int ix = (int)ux, iy = (int)uy, iz = (int)uz;
+    if (ux < 0) ix--;
+    if (uy < 0) iy--;
+    const double tx = ux - ix, ty = uy - iy, tz = uz - iz;
+    if (iz < 3) iz = 3; else if (iz > nz - 5) iz = nz - 5;   /* _clamp(iz,3,n.z-5) */
+    ix = modulo_i(ix - 1, nx);
+    iy = modulo_i(iy - 1, ny);
+    const int nyz = nz * ny;
+    int qx[4], qy[4];
+    choose_inds_pbc(ix, nx, qx);
+    choose_inds_pbc(iy, ny, qy);
+    for (int k = 0; k < 4; k++) { qx[k] *= nyz; qy[k] *= nz; }
+    double bz[4], dz[4], by[4], dy[4], bx[4], dx[4];
+    bs_basis(tz, bz); bs_dbasis(tz, dz);
+    bs_basis(ty, by); bs_dbasis(ty, dy);
+    const int i0 = (iz - 1) + nz * (iy + ny * ix);
+    double Ex[4], Ey[4], Ez[4];
+    for (int a = 0; a < 4; a++) {
+        const int base = i0 + qx[a];
+        double fe0[4], fe1[4];   /* per y-column: (value, d/dz) */
+        for (int b = 0; b < 4; b++) {
+            const double* E = C + 3 * (base + qy[b]);
+            double cs[4];
+            for (int k = 0; k < 4; k++) {
+                const double* e = E + 3 * k;
+                cs[k] = PLQ[0] * e[0] + PLQ[1] * e[1] + PLQ[2] * e[2];
+            }
+            fe0[b] = bz[0] * cs[0] + bz[1] * cs[1] + bz[2] * cs[2] + bz[3] * cs[3];
+            fe1[b] = dz[0] * cs[0] + dz[1] * cs[1] + dz[2] * cs[2] + dz[3] * cs[3];
+        }
+        Ex[a] = fe0[0] * dy[0] + fe0[1] * dy[1] + fe0[2] * dy[2] + fe0[3] * dy[3];
+        Ey[a] = fe1[0] * by[0] + fe1[1] * by[1] + fe1[2] * by[2] + fe1[3] * by[3];
+        Ez[a] = fe0[0] * by[0] + fe0[1] * by[1] + fe0[2] * by[2] + fe0[3] * by[3];
+    }
+    bs_basis(tx, bx); bs_dbasis(tx, dx);
+    double Fx = dx[0] * Ez[0] + dx[1] * Ez[1] + dx[2] * Ez[2] + dx[3] * Ez[3];
+    double Fy = bx[0] * Ex[0] + bx[1] * Ex[1] + bx[2] * Ex[2] + bx[3] * Ex[3];
+    double Fz = bx[0] * Ey[0] + bx[1] * Ey[1] + bx[2] * Ey[2] + bx[3] * Ey[3];
+    double Ee = bx[0] * Ez[0] + bx[1] * Ez[1] + bx[2] * Ez[2] + bx[3] * Ez[3];
+    fe[0] = Fx * (-1.0 / step[0]);
+    fe[1] = Fy * (-1.0 / step[1]);
+    fe[2] = Fz * (-1.0 / step[2]);
+    fe[3] = Ee;
+}
+
+/* Forces.h:611 REQ2PLQ_d */
+static inline void req2plq(const double* REQ, double K, double* PLQ) {
+    double e = exp(K * REQ[0]);
+    double cL = e * REQ[1];
+    double cP = e * cL;
+    double cH = e * e * REQ[3];
+    PLQ[0] = cP; PLQ[1] = cL; PLQ[2] = REQ[2]; PLQ[3] = cH;
+}
+
+void orc_req2plq(int n, const double* REQ, double K, double* PLQ) {
+    for (int i = 0; i < n; i++) req2plq(REQ + 4 * i, K, PLQ + 4 * i);
+}
+
+void orc_grid_sample(int n, const double* pos, const double* PLQ, const double* gridC,
+                     const ORC_params* P, double* fe) {
+    for (int i = 0; i < n; i++) {
+        grid_fe(gridC, P->gn, P->gpos0, P->gstep, ld3(pos + 3 * i), PLQ + 4 * i, fe + 4 * i);
+    }
+}
+
+/* ---------------- one force evaluation of a system ---------------- */
+
+/* Force phase of MolWorld_sp3::run_no_omp (MolWorld_sp3.h:2305-2386):
+ * per atom: clear, eval_atom (nodes), evalLJQs_ng4_PBC_atom_omp, gridFF.addAtom;
+ * then assemble_atom for all atoms (MMFFsp3_loc.h:997-1021). */
+static void eval_system(sysview* S, const ORC_params* P, const double* gridC, double* Eparts) {
+    double Eb = 0, Enb = 0, Eg = 0;
+    for (int ia = 0; ia < S->natoms; ia++) {
+        st3(S->force + 3 * ia, v3make(0, 0, 0));
+        if (ia < S->nnode) st3(S->force + 3 * (ia + S->natoms), v3make(0, 0, 0));
+        if (ia < S->nnode) Eb += eval_atom(S, P, ia);
+        if (P->flags & ORC_NONBONDED) Enb += eval_nb_atom(S, P, ia);
+        if (P->flags & ORC_GRID) {
+            double PLQ[4], fe[4];
+            req2plq(S->REQs + 4 * ia, P->alphaMorse, PLQ);
+            grid_fe(gridC, P->gn, P->gpos0, P->gstep, ld3(S->pos + 3 * ia), PLQ, fe);
+            double* f = S->force + 3 * ia;
+            f[0] += fe[0]; f[1] += fe[1]; f[2] += fe[2];
+            Eg += fe[3];
+        }
+    }
+    /* assemble_atom */
+    for (int ia = 0; ia < S->natoms; ia++) {
+        v3 fa = v3make(0, 0, 0), fp = v3make(0, 0, 0);
+        const int* ings = S->bkneighs + 4 * ia;
+        int bpi = ia < S->nnode;
+        for (int i = 0; i < 4; i++) {
+            int j = ings[i];
+            if (j < 0) break;
+            fa = vadd(fa, ld3(S->fneigh + 3 * j));
+            if (bpi) fp = vadd(fp, ld3(S->fneighpi + 3 * j));
+        }
+        double* f = S->force + 3 * ia;
+        st3(f, vadd(ld3(f), fa));
+        if (bpi) {
+            double* fq = S->force + 3 * (S->natoms + ia);
+            v3 fpv = vadd(ld3(fq), fp);
+            v3 u = ld3(S->pos + 3 * (S->natoms + ia));
+            double c = vdot(fpv, u);          /* Vec3::makeOrthoU */
+            fpv = vaddmul(fpv, u, -c);
+            st3(fq, fpv);
+        }
+    }
+    Eparts[0] = Eb; Eparts[1] = Enb; Eparts[2] = Eg; Eparts[3] = Eb + Enb + Eg;
+}
+
+typedef struct {
+    int* aoff; int* noff; int* voff;
+} offsets_t;
+
+static offsets_t make_offsets(int nsys, const int* natoms, const int* nnode) {
+    offsets_t o;
+    o.aoff = (int*)malloc(sizeof(int) * (nsys + 1));
+    o.noff = (int*)malloc(sizeof(int) * (nsys + 1));
+    o.voff = (int*)malloc(sizeof(int) * (nsys + 1));
+    o.aoff[0] = o.noff[0] = o.voff[0] = 0;
+    for (int s = 0; s < nsys; s++) {
+        o.aoff[s + 1] = o.aoff[s] + natoms[s];
+        o.noff[s + 1] = o.noff[s] + nnode[s];
+        o.voff[s + 1] = o.voff[s] + natoms[s] + nnode[s];
+    }
+    return o;
+}
+static void free_offsets(offsets_t o) { free(o.aoff); free(o.noff); free(o.voff); }
+
+static void setup_view(sysview* S, int s, const offsets_t* o, const int* natoms, const int* nnode,
+                       const double* pos, double* force,
+                       const int* neighs, const int* neighCell, const int* bkneighs,
+                       const double* REQs, const double* apars, const double* bLs,
+                       const double* bKs, const double* Ksp, const double* Kpp,
+                       const double* lvec, const ORC_params* P) {
+    S->natoms = natoms[s]; S->nnode = nnode[s]; S->nvecs = natoms[s] + nnode[s];
+    S->pos = pos + 3 * o->voff[s];
+    S->force = force + 3 * o->voff[s];
+    S->neighs = neighs + 4 * o->aoff[s];
+    S->neighCell = neighCell + 4 * o->aoff[s];
+    S->bkneighs = bkneighs + 4 * o->aoff[s];
+    S->REQs = REQs + 4 * o->aoff[s];
+    S->apars = apars + 4 * o->noff[s];
+    S->bLs = bLs + 4 * o->noff[s];
+    S->bKs = bKs + 4 * o->noff[s];
+    S->Ksp = Ksp + 4 * o->noff[s];
+    S->Kpp = Kpp + 4 * o->noff[s];
+    S->lvec = lvec + 9 * s;
+    S->npbc = (2 * P->npbc[0] + 1) * (2 * P->npbc[1] + 1) * (2 * P->npbc[2] + 1);
+    S->shifts = (v3*)malloc(sizeof(v3) * S->npbc);
+    for (int k = 0; k < S->npbc; k++) S->shifts[k] = pbc_shift(S->lvec, P->npbc, k);
+    S->fneigh = (double*)calloc((size_t)S->nnode * 12 + 12, sizeof(double));
+    S->fneighpi = (double*)calloc((size_t)S->nnode * 12 + 12, sizeof(double));
+}
+static void free_view(sysview* S) { free(S->shifts); free(S->fneigh); free(S->fneighpi); }
+
+void orc_eval(int nsys, const int* natoms, const int* nnode,
+              const double* pos, double* force, double* Es,
+              const int* neighs, const int* neighCell, const int* bkneighs,
+              const double* REQs, const double* apars, const double* bLs,
+              const double* bKs, const double* Ksp, const double* Kpp,
+              const double* lvec, const double* gridC, const ORC_params* P, int nthreads) {
+    offsets_t o = make_offsets(nsys, natoms, nnode);
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 1)
+#endif
+    for (int s = 0; s < nsys; s++) {
+        sysview S;
+        setup_view(&S, s, &o, natoms, nnode, pos, force, neighs, neighCell, bkneighs, REQs,
+                   apars, bLs, bKs, Ksp, Kpp, lvec, P);
+        eval_system(&S, P, gridC, Es + 4 * s);
+        free_view(&S);
+    }
+    free_offsets(o);
+}
+
+/* DynamicOpt.cpp:250-267 FIRE_update_params, then MMFFsp3_loc.h:1264-1281
+ * move_atom_FIRE for every vector, as called from MolWorld_sp3::run_no_omp
+ * (MolWorld_sp3.h:2401-2430): move_atom_FIRE(i, (float)opt.dt, 1e4, opt.cv,
+ * opt.renorm_vf*opt.cf). */
+void orc_relax(int nsys, const int* natoms, const int* nnode,
+               double* pos, double* vel, double* fire_state,
+               const int* neighs, const int* neighCell, const int* bkneighs,
+               const double* REQs, const double* apars, const double* bLs,
+               const double* bKs, const double* Ksp, const double* Kpp,
+               const double* lvec, const double* gridC, const ORC_params* P,
+               const ORC_fire* F, int niter, double Fconv, int conv_mode,
+               int* nsteps_out, int* conv_out, double* Fout, double* Eout, int nthreads) {
+    offsets_t o = make_offsets(nsys, natoms, nnode);
+    size_t nvtot = (size_t)o.voff[nsys];
+    double* force = (double*)calloc(nvtot * 3 + 3, sizeof(double));
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 1)
+#endif
+    for (int s = 0; s < nsys; s++) {
+        sysview S;
+        setup_view(&S, s, &o, natoms, nnode, pos, force, neighs, neighCell, bkneighs, REQs,
+                   apars, bLs, bKs, Ksp, Kpp, lvec, P);
+        double* p = pos + 3 * o.voff[s];
+        double* v = vel + 3 * o.voff[s];
+        double* fst = fire_state + 4 * s;
+        double dt = fst[0], damping = fst[1];
+        int lastNeg = (int)fst[2];
+        const double F2conv = Fconv * Fconv;
+        int itr;
+        int conv = 0;
+        double meas = 0;
+        double Ep[4] = {0, 0, 0, 0};
+        const int nv = S.nvecs;
+        for (itr = 0; itr < niter; itr++) {
+            eval_system(&S, P, gridC, Ep);
+            double vf = 0, vv = 0, ff = 0, fmax2 = 0;
+            for (int i = 0; i < nv; i++) {
+                for (int k = 0; k < 3; k++) {
+                    double vi = v[3 * i + k], fi = S.force[3 * i + k];
+                    vf += vi * fi; vv += vi * vi; ff += fi * fi;
+                }
+                double f2 = S.force[3 * i] * S.force[3 * i] + S.force[3 * i + 1] * S.force[3 * i + 1] +
+                            S.force[3 * i + 2] * S.force[3 * i + 2];
+                if (f2 > fmax2) fmax2 = f2;
+            }
+            /* FIRE_update_params */
+            double f_len = sqrt(ff), v_len = sqrt(vv);
+            double cos_vf = vf / (f_len * v_len + 1e-32);
+            double renorm_vf = v_len / (f_len + 1e-32);
+            double cv, cf;
+            if (cos_vf < 0.0) { cv = F->cv_kill; cf = 0.; } else { cv = 1 - damping; cf = damping; }
+            cf = renorm_vf * cf;
+            if (cos_vf < 0.0) {
+                dt = fmax(dt * F->fdec, F->dt_min);
+                lastNeg = 0;
+                damping = F->damp_max;
+            } else {
+                if (lastNeg > F->minLastNeg) {
+                    dt = fmin(dt * F->finc, F->dt_max);
+                    damping = damping * F->falpha;
+                }
+                lastNeg++;
+            }
+            /* move_atom_FIRE(i, (float)dt, Flim, cv, renorm_vf*cf) */
+            const double dtf = (double)(float)dt;
+            const double cfm = renorm_vf * cf;
+            for (int i = 0; i < nv; i++) {
+                v3 f = ld3(S.force + 3 * i), vi = ld3(v + 3 * i), pi = ld3(p + 3 * i);
+                const int bPi = i >= S.natoms;
+                if (bPi) f = vaddmul(f, pi, -vdot(pi, f));
+                vi = vmul(vi, cv);
+                vi = vaddmul(vi, f, dtf + cfm);
+                if (bPi) vi = vaddmul(vi, pi, -vdot(pi, vi));
+                pi = vaddmul(pi, vi, dtf);
+                if (bPi) {
+                    double l = sqrt(pi.x * pi.x + pi.y * pi.y + pi.z * pi.z);
+                    pi = vmul(pi, 1.0 / l);
+                }
+                st3(p + 3 * i, pi); st3(v + 3 * i, vi);
+            }
+            meas = (conv_mode == 0) ? ff : fmax2;
+            double thr = F2conv;
+            if (meas < thr) { conv = 1; break; }
+        }
+        fst[0] = dt; fst[1] = damping; fst[2] = (double)lastNeg;
+        nsteps_out[s] = itr;
+        conv_out[s] = conv;
+        Fout[s] = sqrt(meas);
+        if (Eout) { for (int k = 0; k < 4; k++) Eout[4 * s + k] = Ep[k]; }
+        free_view(&S);
+    }
+    free(force);
+    free_offsets(o);
+}
+
+/* ---------------- grid construction (GridFF.h:582-635, 847-891) ---------------- */
+
+void orc_grid_potentials(int nsub, const double* spos, const double* sREQ,
+                         const double* lvec, const int* nPBC_mors, const int* nPBC_coul,
+                         const ORC_params* P, double* V, int nthreads) {
+    const int nx = P->gn[0], ny = P->gn[1], nz = P->gn[2];
+    const int nm = (2 * nPBC_mors[0] + 1) * (2 * nPBC_mors[1] + 1) * (2 * nPBC_mors[2] + 1);
+    const int nc = (2 * nPBC_coul[0] + 1) * (2 * nPBC_coul[1] + 1) * (2 * nPBC_coul[2] + 1);
+    v3* sm = (v3*)malloc(sizeof(v3) * nm);
+    v3* sc = (v3*)malloc(sizeof(v3) * nc);
+    for (int k = 0; k < nm; k++) sm[k] = pbc_shift(lvec, nPBC_mors, k);
+    for (int k = 0; k < nc; k++) sc[k] = pbc_shift(lvec, nPBC_coul, k);
+    const double K = -P->alphaMorse;
+    const long ntot = (long)nx * ny * nz;
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(static)
+#endif
+    for (long i = 0; i < ntot; i++) {
+        int iz = (int)(i % nz);
+        int iy = (int)((i / nz) % ny);
+        int ix = (int)(i / ((long)nz * ny));
+        v3 pos = v3make(P->gpos0[0] + P->gstep[0] * ix, P->gpos0[1] + P->gstep[1] * iy,
+                        P->gpos0[2] + P->gstep[2] * iz);
+        double vp = 0, vl = 0, vc = 0;
+        for (int ia = 0; ia < nsub; ia++) {
+            v3 dp0 = vsub(pos, ld3(spos + 3 * ia));
+            const double* R = sREQ + 4 * ia;
+            for (int k = 0; k < nm; k++) {
+                v3 dp = vadd(dp0, sm[k]);
+                double r2 = vdot(dp, dp);
+                double r = sqrt(r2 + 1e-32);
+                double e = exp(K * (r - R[0]));
+                double eM = e * R[1];
+                vp += eM * e;
+                vl += eM * -2.;
+            }
+            for (int k = 0; k < nc; k++) {
+                v3 dp = vadd(dp0, sc[k]);
+                double r2 = vdot(dp, dp);
+                double ir2 = 1 / (r2 + 1e-32);
+                vc += COULOMB_CONST * R[2] * sqrt(ir2);
+            }
+        }
+        V[3 * i] = vp; V[3 * i + 1] = vl; V[3 * i + 2] = vc;
+    }
+    free(sm); free(sc);
+}
+
+/* 1-D solves of (c[i-1] + 4 c[i] + c[i+1]) / 6 = v[i] */
+static void solve_periodic(int n, double* x, double* work) {
+    /* circulant tridiagonal, Sherman-Morrison on the Thomas algorithm */
+    const double a = 1.0 / 6.0, b = 4.0 / 6.0;
+    double* cp = work;            /* n */
+    double* u = work + n;         /* n */
+    double* z = work + 2 * n;     /* n */
+    double gamma = -b;
+    double bb0 = b - gamma;
+    double bbn = b - a * a / gamma;
+    /* solve T y = x and T z = u, T = tridiag with modified ends */
+    for (int i = 0; i < n; i++) u[i] = 0;
+    u[0] = gamma; u[n - 1] = a;
+    double* rhs[2] = {x, u};
+    double* out[2] = {x, z};
+    for (int r = 0; r < 2; r++) {
+        double* d = rhs[r];
+        double* y = out[r];
+        if (r == 1) for (int i = 0; i < n; i++) y[i] = d[i];
+        double diag0 = bb0;
+        cp[0] = a / diag0;
+        y[0] = y[0] / diag0;
+        for (int i = 1; i < n; i++) {
+            double diag = (i == n - 1 ? bbn : b) - a * cp[i - 1];
+            cp[i] = a / diag;
+            y[i] = (y[i] - a * y[i - 1]) / diag;
+        }
+        for (int i = n - 2; i >= 0; i--) y[i] -= cp[i] * y[i + 1];
+    }
+    double fact = (x[0] + a * x[n - 1] / gamma) / (1.0 + z[0] + a * z[n - 1] / gamma);
+    for (int i = 0; i < n; i++) x[i] -= fact * z[i];
+}
+static void solve_open(int n, double* y, double* cp) {
+    const double a = 1.0 / 6.0, b = 4.0 / 6.0;
+    cp[0] = a / b;
+    y[0] = y[0] / b;
+    for (int i = 1; i < n; i++) {
+        double diag = b - a * cp[i - 1];
+        cp[i] = a / diag;
+        y[i] = (y[i] - a * y[i - 1]) / diag;
+    }
+    for (int i = n - 2; i >= 0; i--) y[i] -= cp[i] * y[i + 1];
+}
+
+void orc_bspline_fit(const int* gn, const double* V, double* C) {
+    const int nx = gn[0], ny = gn[1], nz = gn[2];
+    const long ntot = (long)nx * ny * nz;
+    memcpy(C, V, sizeof(double) * 3 * ntot);
+    int nmax = nx > ny ? nx : ny; if (nz > nmax) nmax = nz;
+    double* line = (double*)malloc(sizeof(double) * nmax);
+    double* work = (double*)malloc(sizeof(double) * 3 * nmax);
+    for (int ch = 0; ch < 3; ch++) {
+        /* z (open) */
+        for (int ix = 0; ix < nx; ix++) for (int iy = 0; iy < ny; iy++) {
+            long b = ((long)ix * ny + iy) * nz;
+            for (int k = 0; k < nz; k++) line[k] = C[3 * (b + k) + ch];
+            solve_open(nz, line, work);
+            for (int k = 0; k < nz; k++) C[3 * (b + k) + ch] = line[k];
+        }
+        /* y (periodic) */
+        for (int ix = 0; ix < nx; ix++) for (int iz = 0; iz < nz; iz++) {
+            for (int k = 0; k < ny; k++) line[k] = C[3 * (((long)ix * ny + k) * nz + iz) + ch];
+            solve_periodic(ny, line, work);
+            for (int k = 0; k < ny; k++) C[3 * (((long)ix * ny + k) * nz + iz) + ch] = line[k];
+        }
+        /* x (periodic) */
+        for (int iy = 0; iy < ny; iy++) for (int iz = 0; iz < nz; iz++) {
+            for (int k = 0; k < nx; k++) line[k] = C[3 * (((long)k * ny + iy) * nz + iz) + ch];
+            solve_periodic(nx, line, work);
+            for (int k = 0; k < nx; k++) C[3 * (((long)k * ny + iy) * nz + iz) + ch] = line[k];
+        }
+    }
+    free(line); free(work);
+}

@@ -1,0 +1,115 @@
+/*
+ * mmff_oracle.h -- FP64 CPU restatement of FireCore's multi-system MMFF
+ * relaxation hot path.  TEST INFRASTRUCTURE ONLY: this code is the checker
+ * that the CUDA path is compared against.  Only tests/, __graft_entry__.smoke()
+ * and bench.py's cpu_baseline / reference arm may load it; the product library
+ * never links it and has no CPU fallback.
+ *
+ * Parity pin: the restatement is validated against the reference's own C++
+ * physics (MMFFsp3_loc::eval_atom, NBFF::evalLJQs_ng4_PBC_atom_omp,
+ * GridFF::getForce_Bspline, DynamicOpt::FIRE_update_params,
+ * MMFFsp3_loc::move_atom_FIRE driven as in MolWorld_sp3::run_no_omp),
+ * compiled from the reference sources by oracle/Makefile into oracle/_ref,
+ * through the golden fixtures in tests/golden/.
+ *
+ * Layout (all arrays FP64 / int32, systems packed back to back, CSR):
+ *   system s has natoms[s] atoms (nnode[s] node atoms first, then caps) and
+ *   nvecs = natoms + nnode vectors (atoms, then one pi-orbital per node).
+ *   pos/vel/force : [sum nvecs][3]
+ *   neighs/neighCell/bkneighs : [sum natoms][4]  (indices local to the system,
+ *       bkneighs values are ia*4+j into the node recoil slots, as produced by
+ *       MMFFsp3_loc::makeBackNeighs, cpp/common/molecular/MMFFsp3_loc.h:1336)
+ *   REQs  : [sum natoms][4]  (R0, sqrt(E0), Q, H)
+ *   apars/bLs/bKs/Ksp/Kpp : [sum nnode][4]
+ *   lvec  : [nsys][9] (rows a,b,c)
+ *   grid coefficients : [nx][ny][nz][3] z-fastest, channels (Pauli, London, Coulomb)
+ */
+#ifndef MMFF_ORACLE_H
+#define MMFF_ORACLE_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* flag bits for ORC_params.flags */
+enum {
+    ORC_BONDS        = 1 << 0,
+    ORC_PIPI         = 1 << 1,
+    ORC_PISIGMA      = 1 << 2,
+    ORC_ANGLES       = 1 << 3,
+    ORC_SUB_ANGLE_NB = 1 << 4,   /* bSubtractAngleNonBond */
+    ORC_SUB_BOND_NB  = 1 << 5,   /* bSubtractBondNonBond  */
+    ORC_CLAMP_NB     = 1 << 6,   /* bClampNonBonded       */
+    ORC_NONBONDED    = 1 << 7,
+    ORC_GRID         = 1 << 8,
+    ORC_PBC          = 1 << 9,
+};
+
+/* Scalar parameters shared by every system of a call. */
+typedef struct {
+    int    flags;
+    int    npbc[3];        /* nPBC image counts, images run -n..n        */
+    double Rcut;           /* <=0: no cutoff (reference semantics)      */
+    double Ron;            /* switching starts here (Ron<Rcut)          */
+    double FmaxNonBonded;  /* clamp for bClampNonBonded                 */
+    double alphaMorse;     /* REQ -> PLQ conversion exponent            */
+    /* grid */
+    int    gn[3];
+    double gpos0[3];
+    double gstep[3];       /* orthorhombic voxel edges                  */
+} ORC_params;
+
+/* FIRE parameters (DynamicOpt members used by FIRE_update_params) */
+typedef struct {
+    double dt_max, dt_min, damp_max, finc, fdec, falpha, cv_kill;
+    int    minLastNeg;
+} ORC_fire;
+
+/* Forces + energies for every system.
+ * Es[s*4+k]: 0 bonded (eval_atom sum), 1 non-bonded (0.5*sum, as the
+ * reference returns), 2 grid, 3 total. */
+void orc_eval(int nsys, const int* natoms, const int* nnode,
+              const double* pos, double* force, double* Es,
+              const int* neighs, const int* neighCell, const int* bkneighs,
+              const double* REQs, const double* apars, const double* bLs,
+              const double* bKs, const double* Ksp, const double* Kpp,
+              const double* lvec, const double* gridC, const ORC_params* P,
+              int nthreads);
+
+/* FIRE relaxation of every system, MolWorld_sp3::run_no_omp semantics.
+ * fire_state[s*4]: dt, damping, lastNeg (as double), unused.
+ * conv_mode 0: sum_DOF f^2 < Fconv^2 (reference); 1: max_vec |f| < Fconv.
+ * nsteps_out[s]: steps done (the reference's return value), conv_out[s]:
+ * 1 if converged. Fout[s]: the convergence measure at exit. */
+void orc_relax(int nsys, const int* natoms, const int* nnode,
+               double* pos, double* vel, double* fire_state,
+               const int* neighs, const int* neighCell, const int* bkneighs,
+               const double* REQs, const double* apars, const double* bLs,
+               const double* bKs, const double* Ksp, const double* Kpp,
+               const double* lvec, const double* gridC, const ORC_params* P,
+               const ORC_fire* F, int niter, double Fconv, int conv_mode,
+               int* nsteps_out, int* conv_out, double* Fout, double* Eout,
+               int nthreads);
+
+/* B-spline GridFF sample of n points: fe[i*4] = (Fx,Fy,Fz,E) for PLQ[i*4]. */
+void orc_grid_sample(int n, const double* pos, const double* PLQ,
+                     const double* gridC, const ORC_params* P, double* fe);
+
+/* REQ -> PLQ (Forces.h REQ2PLQ_d) */
+void orc_req2plq(int n, const double* REQ, double K, double* PLQ);
+
+/* Substrate potentials on grid nodes (GridFF::evalBsplineRef semantics with
+ * bUseEwald=false): V[i*3+c], node order z-fastest. */
+void orc_grid_potentials(int nsub, const double* spos, const double* sREQ,
+                         const double* lvec, const int* nPBC_mors,
+                         const int* nPBC_coul, const ORC_params* P,
+                         double* V, int nthreads);
+
+/* Exact cubic B-spline interpolation coefficients: periodic in x,y, zero
+ * coefficients outside [0,nz) in z (the converged limit of
+ * Bspline::fit3D_omp with bPBC=true).  V and C: [nx][ny][nz][3]. */
+void orc_bspline_fit(const int* gn, const double* V, double* C);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
