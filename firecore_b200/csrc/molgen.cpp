@@ -21,6 +21,7 @@
 #include <vector>
 #include <algorithm>
 #include <array>
+#include <unordered_map>
 #include "mmff_host.h"
 
 namespace {
@@ -140,11 +141,16 @@ void composition(int N, int& nC, int& nN, int& nO, int& nH) {
     if (nC < 1) { nC = 1; nN = std::max(0, nh - 1 - nO); nO = nh - nC - nN; }
 }
 
+// Heavy-atom tree grown on a diamond lattice (bond 1.40 A): every site has four
+// tetrahedral neighbour directions, so bond angles start at 109.47 deg and all
+// torsions are staggered.  A site is occupied only if exactly one of its lattice
+// neighbours is occupied (its parent), so every lattice-adjacent pair is a bond
+// and every 2.29 A pair is a true 1-3 pair.  Hydrogens point into empty sites
+// that touch no other heavy atom and no other hydrogen.
 bool build_mol(int N, Rng& rng, Mol& M, bool hbond) {
     int nC, nN, nO, nH;
     composition(N, nC, nN, nO, nH);
     const int nh = nC + nN + nO;
-    // heavy elements: root is carbon, the rest shuffled
     std::vector<int> hel;
     for (int i = 0; i < nC; i++) hel.push_back(EL_C);
     for (int i = 0; i < nN; i++) hel.push_back(EL_N);
@@ -154,84 +160,136 @@ bool build_mol(int N, Rng& rng, Mol& M, bool hbond) {
     M.el.assign(N, EL_H);
     for (int i = 0; i < nh; i++) M.el[i] = hel[i];
     M.pos.assign(N + nh, V3{0, 0, 0});
-    // Geometric growth: every heavy atom owns 4 tetrahedral bond slots (slot 0
-    // points to its parent); new heavy atoms and then hydrogens occupy free
-    // slots that do not clash with anything placed so far.
-    std::vector<std::array<V3, 4>> slot(nh);
-    std::vector<std::array<char, 4>> used(nh);
     std::vector<std::vector<int>> nb(N);
-    auto make_slots = [&](int a, V3 u) {
-        V3 w = any_perp(u);
-        double tors = rng.uni() * 2.0 * M_PI;
-        V3 w2 = unit(w * std::cos(tors) + cross(u, w) * std::sin(tors));
-        V3 d[4];
-        ideal_dirs(4, 109.47, d);
-        for (int k = 0; k < 4; k++) slot[a][k] = to_frame(d[k], u, w2);
-        used[a] = {0, 0, 0, 0};
+    // lattice bookkeeping
+    struct Site { int x, y, z; };
+    auto key = [](int x, int y, int z) -> uint64_t {
+        return ((uint64_t)(uint32_t)(x + (1 << 20)) << 42) | ((uint64_t)(uint32_t)(y + (1 << 20)) << 21) | (uint64_t)(uint32_t)(z + (1 << 20));
     };
-    auto clash = [&](V3 q, int skip, int nplaced_heavy, int nplaced_h, double rh, double rH) {
-        for (int c = 0; c < nplaced_heavy; c++) {
-            if (c == skip) continue;
-            V3 dd = q - M.pos[c];
-            if (dot(dd, dd) < rh * rh) return true;
-        }
-        for (int c = nh; c < nh + nplaced_h; c++) {
-            V3 dd = q - M.pos[c];
-            if (dot(dd, dd) < rH * rH) return true;
-        }
-        return false;
+    std::unordered_map<uint64_t, int> occ;      // site -> heavy atom
+    std::unordered_map<uint64_t, int> hclaim;   // site claimed by a hydrogen
+    std::vector<Site> site(nh);
+    auto dirs = [](const Site& s, int k, int& dx, int& dy, int& dz) {
+        static const int D[4][3] = {{1, 1, 1}, {1, -1, -1}, {-1, 1, -1}, {-1, -1, 1}};
+        int sg = ((s.x & 1) == 0) ? 1 : -1;   // sublattice A (even) / B (odd)
+        dx = sg * D[k][0]; dy = sg * D[k][1]; dz = sg * D[k][2];
     };
-    make_slots(0, unit(V3{rng.gauss(), rng.gauss(), rng.gauss()}));
-    used[0][0] = 0;
+    auto n_occ_neigh = [&](int x, int y, int z, int skip) {
+        Site t{x, y, z};
+        int n = 0;
+        for (int k = 0; k < 4; k++) {
+            int dx, dy, dz; dirs(t, k, dx, dy, dz);
+            auto it = occ.find(key(x + dx, y + dy, z + dz));
+            if (it != occ.end() && it->second != skip) n++;
+        }
+        return n;
+    };
+    // hydrogen targets per heavy atom (C <= 2, N, O <= 1), summing to nH
+    std::vector<int> hcount(nh, 0);
+    {
+        std::vector<int> slots;
+        for (int i = 0; i < nh; i++) for (int k = 0; k < (hel[i] == EL_C ? 2 : 1); k++) slots.push_back(i);
+        if ((int)slots.size() < nH) return false;
+        for (int k = (int)slots.size() - 1; k > 0; k--) { int j = rng.below(k + 1); std::swap(slots[k], slots[j]); }
+        for (int k = 0; k < nH; k++) hcount[slots[k]]++;
+    }
+    // Hydrogens are claimed as soon as their heavy atom is placed: a hydrogen
+    // site is an empty lattice site touching only its own heavy atom, with no
+    // other hydrogen site next to it; heavy atoms never move next to a claimed
+    // hydrogen site.
+    std::vector<std::vector<int>> hsites(nh);   // lattice direction index per H
+    auto hsite_ok = [&](int x, int y, int z, int owner) {
+        uint64_t k2 = key(x, y, z);
+        if (occ.count(k2) || hclaim.count(k2)) return false;
+        if (n_occ_neigh(x, y, z, owner) != 0) return false;
+        Site t{x, y, z};
+        for (int q = 0; q < 4; q++) {
+            int ex, ey, ez; dirs(t, q, ex, ey, ez);
+            if (hclaim.count(key(x + ex, y + ey, z + ez))) return false;
+        }
+        return true;
+    };
+    auto claim_H = [&](int a) {
+        int want = hcount[a];
+        int order[4] = {0, 1, 2, 3};
+        for (int k = 3; k > 0; k--) { int j = rng.below(k + 1); std::swap(order[k], order[j]); }
+        std::vector<uint64_t> got;
+        std::vector<int> gotk;
+        for (int kk = 0; kk < 4 && (int)got.size() < want; kk++) {
+            int dx, dy, dz; dirs(site[a], order[kk], dx, dy, dz);
+            int x = site[a].x + dx, y = site[a].y + dy, z = site[a].z + dz;
+            if (!hsite_ok(x, y, z, a)) continue;
+            hclaim[key(x, y, z)] = a;
+            got.push_back(key(x, y, z)); gotk.push_back(order[kk]);
+        }
+        if ((int)got.size() < want) { for (auto g : got) hclaim.erase(g); return false; }
+        hsites[a] = gotk;
+        return true;
+    };
+    site[0] = {0, 0, 0};
+    occ[key(0, 0, 0)] = 0;
+    if (!claim_H(0)) return false;
+    std::vector<int> hdeg(nh, 0);
     for (int i = 1; i < nh; i++) {
         bool ok = false;
-        for (int attempt = 0; attempt < 400 && !ok; attempt++) {
+        for (int attempt = 0; attempt < 4000 && !ok; attempt++) {
+            // parent: the one nearest the lattice origin of three random picks
+            // (keeps big molecules globular); plain random after many failures
             int p = rng.below(i);
-            int val = kValence[hel[p]];
-            int deg = (int)nb[p].size();
-            // keep one valence free on carbon (for H or a pi bond)
-            int cap = (hel[p] == EL_C) ? val - 1 : val;
-            if (deg >= cap) continue;
-            int k = rng.below(4);
-            if (used[p][k]) continue;
-            if (p != 0 && k == 0) continue;         // slot 0 is the bond to the parent
-            double L = 1.40 + 0.05 * (2.0 * rng.uni() - 1.0);
-            V3 q = M.pos[p] + slot[p][k] * L;
-            if (clash(q, p, i, 0, 2.1, 0.0)) { continue; }
-            M.pos[i] = q;
-            used[p][k] = 1;
-            nb[p].push_back(i); nb[i].push_back(p);
-            make_slots(i, unit(M.pos[p] - q));
-            used[i][0] = 1;
+            if (attempt < 2000) {
+                for (int t = 0; t < 2; t++) {
+                    int c = rng.below(i);
+                    long rc = (long)site[c].x * site[c].x + (long)site[c].y * site[c].y + (long)site[c].z * site[c].z;
+                    long rp = (long)site[p].x * site[p].x + (long)site[p].y * site[p].y + (long)site[p].z * site[p].z;
+                    if (rc < rp) p = c;
+                }
+            }
+            if (hdeg[p] + hcount[p] >= kValence[hel[p]]) continue;
+            int k = rng.below(4), dx, dy, dz;
+            dirs(site[p], k, dx, dy, dz);
+            int x = site[p].x + dx, y = site[p].y + dy, z = site[p].z + dz;
+            uint64_t kx = key(x, y, z);
+            if (occ.count(kx) || hclaim.count(kx)) continue;
+            if (n_occ_neigh(x, y, z, p) != 0) continue;   // would close a ring / non-bonded contact
+            {   // no foreign hydrogen site next to the new heavy atom
+                bool bad = false;
+                Site t{x, y, z};
+                for (int q = 0; q < 4 && !bad; q++) {
+                    int ex, ey, ez; dirs(t, q, ex, ey, ez);
+                    auto it = hclaim.find(key(x + ex, y + ey, z + ez));
+                    if (it != hclaim.end()) bad = true;
+                }
+                if (bad) continue;
+            }
+            if (1 + hcount[i] > kValence[hel[i]]) continue;
+            site[i] = {x, y, z};
+            occ[kx] = i;
+            if (!claim_H(i)) { occ.erase(kx); continue; }
+            hdeg[p]++; hdeg[i]++;
+            nb[p].push_back(i); nb[i].insert(nb[i].begin(), p);
             ok = true;
         }
         if (!ok) return false;
     }
-    // hydrogens on free slots
-    {
-        std::vector<std::pair<int, int>> fs;
-        for (int a = 0; a < nh; a++) for (int k = 0; k < 4; k++) if (!used[a][k] && !(a == 0 && false)) fs.push_back({a, k});
-        for (int k = (int)fs.size() - 1; k > 0; k--) { int j = rng.below(k + 1); std::swap(fs[k], fs[j]); }
-        int placedH = 0;
-        for (size_t f = 0; f < fs.size() && placedH < nH; f++) {
-            int a = fs[f].first, k = fs[f].second;
-            if ((int)nb[a].size() >= kValence[hel[a]]) continue;
-            V3 q = M.pos[a] + slot[a][k] * 1.09;
-            if (clash(q, a, nh, placedH, 1.8, 1.6)) continue;
-            int ih = nh + placedH;
-            M.pos[ih] = q;
-            used[a][k] = 1;
+    int ih = nh;
+    for (int a = 0; a < nh; a++) {
+        for (int k : hsites[a]) {
+            int dx, dy, dz; dirs(site[a], k, dx, dy, dz);
             nb[a].push_back(ih); nb[ih].push_back(a);
-            placedH++;
+            M.pos[ih] = V3{(double)dx, (double)dy, (double)dz};   // direction, scaled below
+            ih++;
         }
-        if (placedH < nH) return false;
     }
-    // pi orbitals are stored after the atoms: move H positions to their slots
-    {
-        std::vector<V3> P(N + nh);
-        for (int i = 0; i < nh; i++) P[i] = M.pos[i];
-        for (int i = nh; i < N; i++) P[i] = M.pos[i];
-        M.pos = P;
+    if (ih != N) return false;
+    // 3) coordinates: lattice unit so that bonds are 1.40 A, +-0.05 A jitter
+    const double u = 1.40 / std::sqrt(3.0);
+    for (int i = 0; i < nh; i++) {
+        M.pos[i] = V3{site[i].x * u, site[i].y * u, site[i].z * u} +
+                   V3{0.029 * (2 * rng.uni() - 1), 0.029 * (2 * rng.uni() - 1), 0.029 * (2 * rng.uni() - 1)};
+    }
+    for (int h = nh; h < N; h++) {
+        int a = nb[h][0];
+        M.pos[h] = M.pos[a] + unit(M.pos[h]) * 1.09;
     }
     // hybridisation
     std::vector<int> npi(nh), nbt(nh);
@@ -330,25 +388,43 @@ int mmff_gen_systems(int nsys, const int* natoms, uint64_t seed, int topo_mode,
                      int hbond, double* pos, int* neighs, int* neighCell, int* bkneighs,
                      double* REQs, double* apars, double* bLs, double* bKs, double* Ksp,
                      double* Kpp, int* elements, int central_cell) {
-    size_t ao = 0, no = 0, vo = 0;
-    Mol proto;
-    bool have_proto = false;
+    std::vector<size_t> aoff(nsys + 1, 0), noff(nsys + 1, 0), voff(nsys + 1, 0);
     for (int s = 0; s < nsys; s++) {
+        int nh = mmff_gen_nnode(natoms[s]);
+        aoff[s + 1] = aoff[s] + natoms[s];
+        noff[s + 1] = noff[s] + nh;
+        voff[s + 1] = voff[s] + natoms[s] + nh;
+    }
+    auto build_topo = [&](uint64_t topo_seed, int N, Mol& M) {
+        for (int attempt = 0; attempt < 400; attempt++) {
+            Rng r(topo_seed * 7919ull + (uint64_t)attempt * 104729ull + 17ull);
+            if (build_mol(N, r, M, hbond != 0)) return true;
+        }
+        return false;
+    };
+    Mol proto;
+    if (topo_mode == 0 && nsys > 0) {
+        if (!build_topo(seed, natoms[0], proto)) return -1;
+    }
+    int fail = 0;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int s = 0; s < nsys; s++) {
+        if (fail) continue;
         const int N = natoms[s];
         Mol M;
-        uint64_t topo_seed = (topo_mode == 0) ? seed : seed * 1000003ull + (uint64_t)s;
-        if (topo_mode == 0 && have_proto) {
+        if (topo_mode == 0) {
             M = proto;
-        } else {
-            bool ok = false;
-            for (int attempt = 0; attempt < 400 && !ok; attempt++) {
-                Rng r(topo_seed * 7919ull + (uint64_t)attempt * 104729ull + 17ull);
-                ok = build_mol(N, r, M, hbond != 0);
-            }
-            if (!ok) return -(s + 1);
-            if (topo_mode == 0) { proto = M; have_proto = true; }
+        } else if (!build_topo(seed * 1000003ull + (uint64_t)s, N, M)) {
+#pragma omp critical
+            { if (!fail) fail = s + 1; }
+            continue;
         }
-        if ((int)M.natoms != N) return -(s + 1);
+        if ((int)M.natoms != N) {
+#pragma omp critical
+            { if (!fail) fail = s + 1; }
+            continue;
+        }
+        const size_t ao = aoff[s], no = noff[s], vo = voff[s];
         Rng rp(seed * 2654435761ull + (uint64_t)s * 40503ull + 99991ull);
         const int nh = M.nnode;
         // center, rotate, perturb
@@ -383,6 +459,7 @@ int mmff_gen_systems(int nsys, const int* natoms, uint64_t seed, int topo_mode,
         }
         // back neighbours (MMFFsp3_loc::makeBackNeighs ordering)
         for (int i = 0; i < N; i++) for (int k = 0; k < 4; k++) bkneighs[4 * (ao + i) + k] = -1;
+        bool bad = false;
         for (int ia = 0; ia < nh; ia++) {
             for (int j = 0; j < 4; j++) {
                 int ja = M.neighs[4 * ia + j];
@@ -390,9 +467,14 @@ int mmff_gen_systems(int nsys, const int* natoms, uint64_t seed, int topo_mode,
                 int* bk = bkneighs + 4 * (ao + ja);
                 int k = 0;
                 while (k < 4 && bk[k] >= 0) k++;
-                if (k == 4) return -(s + 1);
+                if (k == 4) { bad = true; break; }
                 bk[k] = ia * 4 + j;
             }
+        }
+        if (bad) {
+#pragma omp critical
+            { if (!fail) fail = s + 1; }
+            continue;
         }
         for (int i = 0; i < nh; i++) for (int k = 0; k < 4; k++) {
             apars[4 * (no + i) + k] = M.apars[4 * i + k];
@@ -401,9 +483,8 @@ int mmff_gen_systems(int nsys, const int* natoms, uint64_t seed, int topo_mode,
             Ksp[4 * (no + i) + k] = M.Ksp[4 * i + k];
             Kpp[4 * (no + i) + k] = M.Kpp[4 * i + k];
         }
-        ao += N; no += nh; vo += N + nh;
     }
-    return 0;
+    return fail ? -fail : 0;
 }
 
 // Rock-salt (001) slab, 'layers' layers below z_top, ncell x ncell conventional

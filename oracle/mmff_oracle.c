@@ -550,6 +550,14 @@ void orc_relax(int nsys, const int* natoms, const int* nnode,
         const int nv = S.nvecs;
         for (itr = 0; itr < niter; itr++) {
             eval_system(&S, P, gridC, Ep);
+            if (F->Flim > 0) {
+                const double Fl2 = F->Flim * F->Flim;
+                for (int i = 0; i < nv; i++) {
+                    double* fi = S.force + 3 * i;
+                    double fr2 = fi[0] * fi[0] + fi[1] * fi[1] + fi[2] * fi[2];
+                    if (fr2 > Fl2) { double c = F->Flim / sqrt(fr2); fi[0] *= c; fi[1] *= c; fi[2] *= c; }
+                }
+            }
             double vf = 0, vv = 0, ff = 0, fmax2 = 0;
             for (int i = 0; i < nv; i++) {
                 for (int k = 0; k < 3; k++) {
@@ -558,7 +566,7 @@ void orc_relax(int nsys, const int* natoms, const int* nnode,
                 }
                 double f2 = S.force[3 * i] * S.force[3 * i] + S.force[3 * i + 1] * S.force[3 * i + 1] +
                             S.force[3 * i + 2] * S.force[3 * i + 2];
-                if (f2 > fmax2) fmax2 = f2;
+                if (f2 > fmax2 || f2 != f2) fmax2 = f2;
             }
             /* FIRE_update_params */
             double f_len = sqrt(ff), v_len = sqrt(vv);
@@ -598,6 +606,7 @@ void orc_relax(int nsys, const int* natoms, const int* nnode,
             meas = (conv_mode == 0) ? ff : fmax2;
             double thr = F2conv;
             if (meas < thr) { conv = 1; break; }
+            if (meas != meas) { conv = -1; break; }   /* NaN: the system blew up */
         }
         fst[0] = dt; fst[1] = damping; fst[2] = (double)lastNeg;
         nsteps_out[s] = itr;

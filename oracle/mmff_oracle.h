@@ -62,6 +62,9 @@ typedef struct {
 typedef struct {
     double dt_max, dt_min, damp_max, finc, fdec, falpha, cv_kill;
     int    minLastNeg;
+    double Flim;   /* >0: per-vector force clamp |f|<=Flim after assembly, as in
+                      relax_multi.cl:980-983 (updateAtomsMMFFf4); <=0: none, as
+                      run_no_omp (MolWorld_sp3.h:2426 passes Flim=1e4, unused) */
 } ORC_fire;
 
 /* Forces + energies for every system.
