@@ -42,3 +42,28 @@ def _declare(lib):
     lib.mmff_gen_systems.restype = c_int
     lib.mmff_gen_slab.argtypes = [c_double, c_int, c_int, c_double, c_double, c_void, c_void, c_void, c_void]
     lib.mmff_gen_slab.restype = c_int
+    lib.mmff_last_error.argtypes = []
+    lib.mmff_last_error.restype = ctypes.c_char_p
+    sig = {
+        "mmff_init_device": [c_int], "mmff_sync": [], "mmff_set_params": [c_int, c_void, c_double, c_double, c_double],
+        "mmff_set_fire": [c_double] * 6 + [c_int, c_double, c_double], "mmff_set_launch": [c_int, c_int],
+        "mmff_grid_upload": [c_int, c_int, c_int, c_void, c_void, c_void],
+        "mmff_grid_build": [c_int, c_void, c_void, c_void, c_void, c_void, c_double, c_int, c_int, c_int, c_void,
+                            c_void, c_void],
+        "mmff_grid_sample": [c_int, c_void, c_void, c_void],
+        "mmff_systems_upload": [c_int] + [c_void] * 14, "mmff_systems_restore": [],
+        "mmff_systems_set_state": [c_void, c_void, c_int], "mmff_eval": [c_int],
+        "mmff_relax": [c_int, c_double, c_int], "mmff_get_forces": [c_void], "mmff_get_energies": [c_void],
+        "mmff_get_state": [c_void] * 6, "mmff_timer_start": [], "mmff_num_buckets": [],
+        "mmff_bucket_info": [c_int, c_void], "mmff_set_counting": [c_int], "mmff_get_counters": [c_void],
+    }
+    for name, args in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = c_int
+    lib.mmff_timer_stop.argtypes = []
+    lib.mmff_timer_stop.restype = c_double
+    lib.mmff_peak_fp32.argtypes = []
+    lib.mmff_peak_fp32.restype = c_double
+    lib.mmff_peak_l2.argtypes = [c_int]
+    lib.mmff_peak_l2.restype = c_double

@@ -1,0 +1,331 @@
+// mmff_device.cuh -- device-side physics of the multi-system MMFF relaxer.
+//
+// Every function restates, in FP32, the reference C++ physics the FP64 oracle
+// (oracle/mmff_oracle.c) follows:
+//   bonded  : MMFFsp3_loc::eval_atom        cpp/common/molecular/MMFFsp3_loc.h:250-575
+//             (Forces.h evalBond :137, evalAngleCosHalf :190, evalAngleCos :217,
+//              evalPiAling :230, getLJQH :341)
+//   pair    : NBFF::evalLJQs_ng4_PBC_atom_omp cpp/common/molecular/NBFF.h:575-618
+//   grid    : Bspline::fe3d_pbc_comb3        cpp/common/math/Bspline.h:742-809
+//             via GridFF::getForce_Bspline    cpp/common/molecular/GridFF.h:355-402
+//   assemble: MMFFsp3_loc::assemble_atom     cpp/common/molecular/MMFFsp3_loc.h:998-1021
+//   FIRE    : DynamicOpt::FIRE_update_params cpp/common/math/DynamicOpt.cpp:250-267
+//             MMFFsp3_loc::move_atom_FIRE    cpp/common/molecular/MMFFsp3_loc.h:1264-1281
+// Precision: forces in FP32; the per-system FIRE sums, the FIRE decision and the
+// convergence test in FP64.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define MMFF_COULOMB 14.3996448915f
+
+namespace mmff {
+
+// ---- flags (same bit meaning as the oracle's ORC_* flags)
+enum : int {
+    F_BONDS = 1 << 0, F_PIPI = 1 << 1, F_PISIGMA = 1 << 2, F_ANGLES = 1 << 3,
+    F_SUB_ANGLE_NB = 1 << 4, F_SUB_BOND_NB = 1 << 5, F_CLAMP_NB = 1 << 6,
+    F_NONBONDED = 1 << 7, F_GRID = 1 << 8, F_PBC = 1 << 9,
+};
+
+// status codes per system
+enum : int { ST_RUNNING = 0, ST_CONVERGED = 1, ST_MAXSTEPS = 2, ST_NAN = -1 };
+
+struct Params {
+    int flags;
+    int npbc[3];
+    float Rc2;           // cutoff^2 (<=0: none)
+    float kq_rc2;        // 1/Rcut^2 for the shifted-force Coulomb
+    float Fmax2NB;       // bClampNonBonded
+    // grid
+    int gn[3];
+    float ginv[3];       // 1/step
+    float gmi[3];        // -1/step
+    const float4* __restrict__ grid;   // [nx][ny][nz] (P, L, Q, 0)
+    // FIRE
+    double dt_max, dt_min, damp_max, finc, fdec, falpha, cv_kill;
+    int minLastNeg;
+    float Flim;          // <=0: no force clamp
+    double Fconv2;
+    int conv_mode;       // 0: sum f^2 ; 1: max |f|^2
+    int nstep_max;       // steps allowed in this call
+};
+
+struct Systems {
+    int nsys;
+    const int4* __restrict__ desc;      // (aoff, noff, voff, natoms)
+    const int* __restrict__ nnode;
+    const float* __restrict__ lvec;     // [nsys*9]
+    const float4* __restrict__ gorg;    // grid offset of the local frame: orig - pos0
+    const float4* __restrict__ REQ;     // (R0, sqrt(E0), Q*sqrt(k_e), Hb)
+    const float4* __restrict__ PLQ;     // (P, L, Q, H) for the grid
+    const int4* __restrict__ neighs;
+    const int4* __restrict__ neighCell;
+    const int4* __restrict__ bkneighs;
+    const float4* __restrict__ apars;
+    const float4* __restrict__ bLs;
+    const float4* __restrict__ bKs;
+    const float4* __restrict__ Ksp;
+    const float4* __restrict__ Kpp;
+    float4* pos;                        // local frame
+    float4* vel;
+    float4* force;                      // assembled forces (written by eval / at exit)
+    double4* fire;                      // (dt, damping, lastNeg, total steps)
+    int* status;
+    int* nsteps;                        // steps done in the last call
+    float* fconv;                       // convergence measure at exit (sqrt)
+    double4* energy;                    // eval only: (bonded, non-bonded, grid, total)
+    unsigned long long* counters;       // counting builds: pair-images, atom grid samples, force evaluations
+};
+
+__device__ __forceinline__ float3 f3(float4 a) { return make_float3(a.x, a.y, a.z); }
+__device__ __forceinline__ float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 operator-(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 operator*(float3 a, float f) { return make_float3(a.x * f, a.y * f, a.z * f); }
+__device__ __forceinline__ float dot3(float3 a, float3 b) { return fmaf(a.x, b.x, fmaf(a.y, b.y, a.z * b.z)); }
+__device__ __forceinline__ float3 fma3(float3 a, float f, float3 c) { return make_float3(fmaf(a.x, f, c.x), fmaf(a.y, f, c.y), fmaf(a.z, f, c.z)); }
+
+// Forces.h:341 getLJQH with undamped Coulomb; REQ holds the pair-mixed values with
+// Q = k_e*Qi*Qj.  Returns the scalar F with f = dp * F (the reference's -F).
+template <bool ENERGY>
+__device__ __forceinline__ float ljqh(float r2, float R0, float E0, float Q, float hw, float& E) {
+    const float ir2 = 1.0f / r2;
+    const float ir = sqrtf(ir2);
+    const float Eel = Q * ir;
+    const float u2 = R0 * R0 * ir2;
+    const float u6 = u2 * u2 * u2;
+    const float vdW = u6 * E0;
+    const float H = u6 * vdW * hw;              // u6*u6*(w<0 ? w*E0 : 0)
+    if (ENERGY) E = fmaf(u6 - 2.f, vdW, Eel + H);
+    return -fmaf(12.f * ir2, fmaf(u6 - 1.f, vdW, H), Eel * ir2);
+}
+
+// ----- bonded terms (one node atom), MMFFsp3_loc::eval_atom
+struct BondedOut {
+    float3 fa, fpi;
+    float3 fbs[4], fps[4];
+    float E;
+};
+
+template <bool ENERGY>
+__device__ __forceinline__ void eval_atom(int ia, int natoms, int nnode, int flags, float Fmax2,
+                                          const float4* sp, const float4* sREQ, int4 ng, int4 ngC,
+                                          float4 apar, float4 bL, float4 bK, float4 ksp, float4 kpp,
+                                          const float* lv, int npx, int npy, int npz, BondedOut& o) {
+    const float3 pa = f3(sp[ia]);
+    const float3 hpi = f3(sp[natoms + ia]);
+    float3 fa = make_float3(0, 0, 0), fpi = make_float3(0, 0, 0);
+    float3 fbs[4], fps[4];
+    float3 hf[4];
+    float he[4];
+    float E = 0.f;
+    const int ings[4] = {ng.x, ng.y, ng.z, ng.w};
+    const int ingC[4] = {ngC.x, ngC.y, ngC.z, ngC.w};
+    const float bLa[4] = {bL.x, bL.y, bL.z, bL.w};
+    const float bKa[4] = {bK.x, bK.y, bK.z, bK.w};
+    const float Kspa[4] = {ksp.x, ksp.y, ksp.z, ksp.w};
+    const float Kppa[4] = {kpp.x, kpp.y, kpp.z, kpp.w};
+#pragma unroll
+    for (int i = 0; i < 4; i++) { fbs[i] = make_float3(0, 0, 0); fps[i] = make_float3(0, 0, 0); hf[i] = make_float3(0, 0, 1); he[i] = 1.f; }
+    int nb = 0;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int ing = ings[i];
+        if (ing < 0) break;
+        nb = i + 1;
+        float3 h = f3(sp[ing]) - pa;
+        if (flags & F_PBC) {
+            // shift of image ingC (NBFF.h:42 ordering: iz outer, iy, ix inner)
+            const int c = ingC[i];
+            const int nx = 2 * npx + 1, ny = 2 * npy + 1;
+            const float ix = (float)(c % nx - npx), iy = (float)((c / nx) % ny - npy), iz = (float)(c / (nx * ny) - npz);
+            h.x += lv[0] * ix + lv[3] * iy + lv[6] * iz;
+            h.y += lv[1] * ix + lv[4] * iy + lv[7] * iz;
+            h.z += lv[2] * ix + lv[5] * iy + lv[8] * iz;
+        }
+        const float l = sqrtf(dot3(h, h));
+        const float il = 1.0f / l;
+        h = h * il;
+        hf[i] = h; he[i] = il;
+        if (ia < ing) {
+            if (flags & F_BONDS) {
+                const float dl = l - bLa[i];
+                const float fr = dl * bKa[i];
+                float3 f1 = h * fr;
+                if (ENERGY) E += fr * dl * 0.5f;
+                if (flags & F_SUB_BOND_NB) {
+                    const float4 Ri = sREQ[ia], Rj = sREQ[ing];
+                    const float hw = fminf(Ri.w * Rj.w, 0.f);
+                    float e;
+                    const float3 dp = h * l;
+                    const float F = ljqh<ENERGY>(l * l, Ri.x + Rj.x, Ri.y * Rj.y, Ri.z * Rj.z, hw, e);
+                    float3 fij = dp * F;
+                    if (flags & F_CLAMP_NB) { float f2 = dot3(fij, fij); if (f2 > Fmax2) fij = fij * sqrtf(Fmax2 / f2); }
+                    if (ENERGY) E -= e;
+                    f1 = f1 - fij;
+                }
+                fbs[i] = fbs[i] - f1; fa = fa + f1;
+            }
+            const float kk = Kppa[i];
+            if ((flags & F_PIPI) && (ing < nnode) && (kk > 1e-6f)) {
+                // Forces.h:230 evalPiAling with ir1 = ir2 = 1
+                const float3 h2 = f3(sp[natoms + ing]);
+                float c = dot3(hpi, h2);
+                const float3 a = fma3(hpi, -c, h2);
+                const float3 b = fma3(h2, -c, hpi);
+                const bool sign = c < 0.f;
+                if (sign) c = -c;
+                if (ENERGY) E += kk * (1.f - c);
+                const float fang = sign ? -kk : kk;
+                fpi = fpi + a * fang;
+                fps[i] = fps[i] + b * fang;
+            }
+        }
+        const float ks = Kspa[i];
+        if ((flags & F_PISIGMA) && (ks > 1e-6f)) {
+            // Forces.h:217 evalAngleCos(hpi, h, 1, 1/l, ksp, piC0)
+            const float c = dot3(hpi, h);
+            const float3 a = fma3(hpi, -c, h);
+            const float3 b = fma3(h, -c, hpi);
+            const float c_ = c - apar.w;
+            if (ENERGY) E += ks * c_ * c_;
+            const float fang = -ks * c_ * 2.f;
+            fpi = fpi + a * fang;
+            const float3 f2 = b * (fang * il);
+            fa = fa - f2;
+            fbs[i] = fbs[i] + f2;
+        }
+    }
+    if (flags & F_ANGLES) {
+        const float ssK = apar.z;
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            if (i >= nb) break;
+#pragma unroll
+            for (int j = i + 1; j < 4; j++) {
+                if (j >= nb) break;
+                // Forces.h:190 evalAngleCosHalf
+                const float3 h = hf[i] + hf[j];
+                float c2 = dot3(h, h) * 0.25f;
+                const float s2 = 1.f - c2 + 1e-14f;
+                const float c = sqrtf(c2);
+                const float s = sqrtf(fmaxf(s2, 0.f));
+                const float csx = fmaf(apar.x, c, apar.y * s);
+                const float csy = fmaf(apar.y, c, -apar.x * s);
+                if (ENERGY) E += ssK * (1.f - csx);
+                float fr = -ssK * csy;
+                c2 *= -2.f;
+                fr = fr / (4.f * c * s);
+                const float fr1 = fr * he[i];
+                const float fr2 = fr * he[j];
+                float3 f1 = make_float3(h.x * fr1 + hf[i].x * (fr1 * c2), h.y * fr1 + hf[i].y * (fr1 * c2), h.z * fr1 + hf[i].z * (fr1 * c2));
+                float3 f2 = make_float3(h.x * fr2 + hf[j].x * (fr2 * c2), h.y * fr2 + hf[j].y * (fr2 * c2), h.z * fr2 + hf[j].z * (fr2 * c2));
+                fa = fa - (f1 + f2);
+                if (flags & F_SUB_ANGLE_NB) {
+                    const int ing = ings[i], jng = ings[j];
+                    const float4 Ri = sREQ[ing], Rj = sREQ[jng];
+                    const float hw = fminf(Ri.w * Rj.w, 0.f);
+                    const float3 dp = hf[j] * (1.f / he[j]) - hf[i] * (1.f / he[i]);
+                    float e;
+                    const float F = ljqh<ENERGY>(dot3(dp, dp), Ri.x + Rj.x, Ri.y * Rj.y, Ri.z * Rj.z, hw, e);
+                    float3 fij = dp * F;
+                    if (flags & F_CLAMP_NB) { float ff = dot3(fij, fij); if (ff > Fmax2) fij = fij * sqrtf(Fmax2 / ff); }
+                    if (ENERGY) E -= e;
+                    f1 = f1 - fij;
+                    f2 = f2 + fij;
+                }
+                fbs[i] = fbs[i] + f1;
+                fbs[j] = fbs[j] + f2;
+            }
+        }
+    }
+    o.fa = fa; o.fpi = fpi;
+#pragma unroll
+    for (int i = 0; i < 4; i++) { o.fbs[i] = fbs[i]; o.fps[i] = fps[i]; }
+    o.E = E;
+}
+
+// ----- cubic B-spline basis (Bspline.h:254, :267)
+__device__ __forceinline__ float4 bs_basis(float u) {
+    const float u2 = u * u, t = 1.f - u;
+    const float inv6 = 1.f / 6.f;
+    return make_float4(inv6 * t * t * t, inv6 * fmaf(3.f * u2, u - 2.f, 4.f), inv6 * fmaf(3.f * u, 1.f + u - u2, 1.f), inv6 * u2 * u);
+}
+__device__ __forceinline__ float4 bs_dbasis(float u) {
+    const float u2 = u * u, t = 1.f - u;
+    return make_float4(-0.5f * t * t, 0.5f * (3.f * u2 - 4.f * u), 0.5f * (-3.f * u2 + 2.f * u + 1.f), 0.5f * u2);
+}
+__device__ __forceinline__ float comp(float4 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w)); }
+
+// One x-slice (a = 0..3) of the 4x4x4 stencil of Bspline::fe3d_pbc_comb3 for
+// grid coordinate u (already in voxel units).  Returns the slice's partial
+// (dE/dx*bx', E-channel combos) as (Fx, Fy, Fz, E) *before* the -1/step scale.
+__device__ __forceinline__ float4 grid_slice(const float4* __restrict__ G, int nx, int ny, int nz, float3 u,
+                                             float4 PLQ, int a) {
+    int ix = (int)u.x, iy = (int)u.y, iz = (int)u.z;
+    if (u.x < 0.f) ix--;
+    if (u.y < 0.f) iy--;
+    const float tx = u.x - (float)ix, ty = u.y - (float)iy, tz = u.z - (float)iz;
+    iz = min(max(iz, 3), nz - 5);
+    ix = ix - 1; ix %= nx; if (ix < 0) ix += nx;
+    iy = iy - 1; iy %= ny; if (iy < 0) iy += ny;
+    // x index of this slice with periodic wrap (Bspline.h:36-53 choose_inds_pbc)
+    int xa = ix + a; if (xa >= nx) xa -= nx;
+    const float4 bz = bs_basis(tz), dz = bs_dbasis(tz);
+    const float4 by = bs_basis(ty), dy = bs_dbasis(ty);
+    float ex = 0.f, ey = 0.f, ez = 0.f;   // per slice: d/dy combo, d/dz combo, value
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+        int yb = iy + b; if (yb >= ny) yb -= ny;
+        const float4* col = G + ((size_t)(xa * ny + yb) * nz + (iz - 1));
+        const float4 c0 = __ldg(col), c1 = __ldg(col + 1), c2 = __ldg(col + 2), c3 = __ldg(col + 3);
+        const float cs0 = fmaf(PLQ.x, c0.x, fmaf(PLQ.y, c0.y, PLQ.z * c0.z));
+        const float cs1 = fmaf(PLQ.x, c1.x, fmaf(PLQ.y, c1.y, PLQ.z * c1.z));
+        const float cs2 = fmaf(PLQ.x, c2.x, fmaf(PLQ.y, c2.y, PLQ.z * c2.z));
+        const float cs3 = fmaf(PLQ.x, c3.x, fmaf(PLQ.y, c3.y, PLQ.z * c3.z));
+        const float v = fmaf(bz.x, cs0, fmaf(bz.y, cs1, fmaf(bz.z, cs2, bz.w * cs3)));
+        const float d = fmaf(dz.x, cs0, fmaf(dz.y, cs1, fmaf(dz.z, cs2, dz.w * cs3)));
+        const float byb = comp(by, b), dyb = comp(dy, b);
+        ex = fmaf(v, dyb, ex);
+        ey = fmaf(d, byb, ey);
+        ez = fmaf(v, byb, ez);
+    }
+    const float4 bx = bs_basis(tx), dx = bs_dbasis(tx);
+    const float bxa = comp(bx, a), dxa = comp(dx, a);
+    return make_float4(dxa * ez, bxa * ex, bxa * ey, bxa * ez);
+}
+
+// ---- shared-memory carve-up of one system (byte offsets)
+struct SmemLayout {
+    int maxNA, maxNN, maxNV, nwarps;
+    // offsets in bytes
+    int pos, vel, fasm, fnb, fgrid, REQ, PLQ, ng, ngC, bk, apar, bL, bK, ksp, kpp, fng, red, total;
+};
+
+__host__ __device__ inline SmemLayout smem_layout(int maxNA, int maxNN, int T) {
+    SmemLayout L;
+    L.maxNA = maxNA; L.maxNN = maxNN; L.maxNV = maxNA + maxNN; L.nwarps = T / 32;
+    int o = 0;
+    auto take = [&](int bytes) { int r = o; o += (bytes + 15) & ~15; return r; };
+    L.pos = take(16 * L.maxNV);
+    L.vel = take(16 * L.maxNV);
+    L.fasm = take(16 * L.maxNV);
+    L.fnb = take(16 * maxNA);
+    L.fgrid = take(16 * maxNA);
+    L.REQ = take(16 * maxNA);
+    L.PLQ = take(16 * maxNA);
+    L.ng = take(16 * maxNA);
+    L.ngC = take(16 * maxNA);
+    L.bk = take(16 * maxNA);
+    L.apar = take(16 * maxNN);
+    L.bL = take(16 * maxNN);
+    L.bK = take(16 * maxNN);
+    L.ksp = take(16 * maxNN);
+    L.kpp = take(16 * maxNN);
+    L.fng = take(16 * 8 * maxNN);
+    L.red = take(128 * L.nwarps + 64);     // per warp: 4 doubles (32 B) at 0, bbox 6 floats at 64*nwarps
+    L.total = o;
+    return L;
+}
+
+}  // namespace mmff

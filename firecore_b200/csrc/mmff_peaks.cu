@@ -1,0 +1,88 @@
+// mmff_peaks.cu -- measured denominators for the roofline fractions that
+// have no published or driver-measured figure on this GPU:
+//   * FP32 CUDA-core FMA throughput: independent FFMA chains on every SM,
+//   * L2 read bandwidth: float4 sweeps over a buffer that stays L2-resident.
+#include <cuda_runtime.h>
+#include <string>
+
+namespace {
+__global__ void ffma_kernel(float* out, int iters, float a, float b) {
+    float x0 = threadIdx.x * 1e-3f, x1 = x0 + 1.f, x2 = x0 + 2.f, x3 = x0 + 3.f;
+    float x4 = x0 + 4.f, x5 = x0 + 5.f, x6 = x0 + 6.f, x7 = x0 + 7.f;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            x0 = fmaf(x0, a, b); x1 = fmaf(x1, a, b); x2 = fmaf(x2, a, b); x3 = fmaf(x3, a, b);
+            x4 = fmaf(x4, a, b); x5 = fmaf(x5, a, b); x6 = fmaf(x6, a, b); x7 = fmaf(x7, a, b);
+        }
+    }
+    const float s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+    if (s == 1.2345f) out[threadIdx.x] = s;   // keeps the chains alive
+}
+
+__global__ void l2_read_kernel(const float4* __restrict__ buf, size_t n, int reps, float* out) {
+    float acc = 0.f;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (int r = 0; r < reps; r++) {
+        for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+            const float4 v = __ldcg(buf + i);
+            acc += v.x + v.y + v.z + v.w;
+        }
+    }
+    if (acc == 1.2345f) out[0] = acc;
+}
+}  // namespace
+
+extern "C" {
+
+// Returns TFLOP/s (2 flops per FFMA) or a negative value on error.
+double mmff_peak_fp32(void) {
+    int dev = 0, nsm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    float* out = nullptr;
+    if (cudaMalloc(&out, 1024 * sizeof(float)) != cudaSuccess) return -1;
+    const int blocks = nsm * 8, threads = 256, iters = 4096;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0); cudaEventCreate(&e1);
+    ffma_kernel<<<blocks, threads>>>(out, 64, 1.0000001f, 1e-7f);   // warm-up
+    cudaEventRecord(e0);
+    ffma_kernel<<<blocks, threads>>>(out, iters, 1.0000001f, 1e-7f);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0); cudaEventDestroy(e1);
+    cudaFree(out);
+    if (cudaGetLastError() != cudaSuccess || ms <= 0.f) return -1;
+    const double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
+    return flops / (ms * 1e-3) / 1e12;
+}
+
+// Returns GB/s of L2-resident float4 reads over a buffer of mbytes MiB.
+double mmff_peak_l2(int mbytes) {
+    int dev = 0, nsm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const size_t n = (size_t)mbytes * (1 << 20) / sizeof(float4);
+    float4* buf = nullptr; float* out = nullptr;
+    if (cudaMalloc(&buf, n * sizeof(float4)) != cudaSuccess) return -1;
+    if (cudaMalloc(&out, sizeof(float)) != cudaSuccess) { cudaFree(buf); return -1; }
+    cudaMemset(buf, 0, n * sizeof(float4));
+    const int blocks = nsm * 8, threads = 512, reps = 20;
+    l2_read_kernel<<<blocks, threads>>>(buf, n, 2, out);   // warm the L2
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0); cudaEventCreate(&e1);
+    cudaEventRecord(e0);
+    l2_read_kernel<<<blocks, threads>>>(buf, n, reps, out);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0); cudaEventDestroy(e1);
+    cudaFree(buf); cudaFree(out);
+    if (cudaGetLastError() != cudaSuccess || ms <= 0.f) return -1;
+    return (double)n * sizeof(float4) * reps / (ms * 1e-3) / 1e9;
+}
+
+}  // extern "C"

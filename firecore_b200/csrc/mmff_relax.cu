@@ -1,0 +1,547 @@
+// mmff_relax.cu -- system-resident relaxation kernels for sm_100a.
+//
+// One CTA owns one system at a time.  The system's whole state (positions,
+// velocities, topology, force-field parameters, recoil slots) is staged in
+// shared memory, and every FIRE step runs inside the CTA:
+//   phase 1  bonded terms (thread per node), non-bonded pairs (S threads per
+//            atom, j-split, warp-shuffle reduction) and the B-spline GridFF
+//            sample (4 lanes per atom, one x-slice of the 4x4x4 stencil each,
+//            float4 gathers that stay resident in L2)
+//   phase 2  recoil assembly (MMFFsp3_loc::assemble_atom), optional force clamp,
+//            FP64 block reduction of (f.v, v.v, f.f) and max|f|^2
+//   phase 3  FIRE_update_params in FP64 (every thread computes the same
+//            scalars), move_atom_FIRE, bounding box for PBC-image culling
+// The persistent variant claims systems from a device work queue (atomic
+// counter): a CTA that finishes a system (converged, failed or out of steps)
+// writes it back and claims the next one, so converged systems retire and
+// their slots refill without a host round trip.
+#include "mmff_device.cuh"
+#include <cfloat>
+
+namespace mmff {
+
+// warp-level sums / extrema
+__device__ __forceinline__ double wsum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float wmax(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ float wmin(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Image shift for cell index (ix, iy, iz)
+__device__ __forceinline__ float3 image_shift(const float* lv, int ix, int iy, int iz) {
+    return make_float3(lv[0] * ix + lv[3] * iy + lv[6] * iz, lv[1] * ix + lv[4] * iy + lv[7] * iz,
+                       lv[2] * ix + lv[5] * iy + lv[8] * iz);
+}
+
+// ---------------------------------------------------------------------------
+// The per-system engine.  T threads, S threads per atom in the pair sum.
+template <int T, int S, bool ENERGY, bool COUNT = false>
+struct Engine {
+    static_assert(T % 32 == 0 && 32 % S == 0, "bad tile");
+    const Params& P;
+    const Systems& Y;
+    SmemLayout L;
+    char* sm;
+    int tid, lane, warp;
+    // current system
+    int isys, natoms, nnode, nvecs, aoff, noff, voff;
+    float lv[9];
+    float3 gorg;
+    // per-step image culling
+    float bbmin[3], bbmax[3];
+    // pair-images evaluated by this thread (COUNT builds only)
+    unsigned long long npair = 0;
+
+    __device__ Engine(const Params& p, const Systems& y, char* smem, const SmemLayout& l)
+        : P(p), Y(y), L(l), sm(smem) {
+        tid = threadIdx.x; lane = tid & 31; warp = tid >> 5;
+    }
+    template <class X> __device__ __forceinline__ X* at(int off) { return reinterpret_cast<X*>(sm + off); }
+
+    __device__ void load(int s) {
+        isys = s;
+        const int4 d = Y.desc[s];
+        aoff = d.x; noff = d.y; voff = d.z; natoms = d.w;
+        nnode = Y.nnode[s];
+        nvecs = natoms + nnode;
+#pragma unroll
+        for (int k = 0; k < 9; k++) lv[k] = Y.lvec[9 * s + k];
+        const float4 g = Y.gorg[s];
+        gorg = make_float3(g.x, g.y, g.z);
+        float4* spos = at<float4>(L.pos); float4* svel = at<float4>(L.vel);
+        for (int v = tid; v < nvecs; v += T) { spos[v] = Y.pos[voff + v]; svel[v] = Y.vel[voff + v]; }
+        float4* sREQ = at<float4>(L.REQ); float4* sPLQ = at<float4>(L.PLQ);
+        int4* sng = at<int4>(L.ng); int4* sngC = at<int4>(L.ngC); int4* sbk = at<int4>(L.bk);
+        for (int a = tid; a < natoms; a += T) {
+            sREQ[a] = Y.REQ[aoff + a]; sPLQ[a] = Y.PLQ[aoff + a];
+            sng[a] = Y.neighs[aoff + a]; sngC[a] = Y.neighCell[aoff + a]; sbk[a] = Y.bkneighs[aoff + a];
+        }
+        float4* sap = at<float4>(L.apar); float4* sbL = at<float4>(L.bL); float4* sbK = at<float4>(L.bK);
+        float4* sks = at<float4>(L.ksp); float4* skp = at<float4>(L.kpp);
+        for (int n = tid; n < nnode; n += T) {
+            sap[n] = Y.apars[noff + n]; sbL[n] = Y.bLs[noff + n]; sbK[n] = Y.bKs[noff + n];
+            sks[n] = Y.Ksp[noff + n]; skp[n] = Y.Kpp[noff + n];
+        }
+    }
+
+    // bounding box of the atoms (all threads end with the same box); needs a barrier inside
+    __device__ void bbox_from_smem() {
+        const float4* spos = at<float4>(L.pos);
+        float mn[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, mx[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+        for (int a = tid; a < natoms; a += T) {
+            const float4 p = spos[a];
+            mn[0] = fminf(mn[0], p.x); mn[1] = fminf(mn[1], p.y); mn[2] = fminf(mn[2], p.z);
+            mx[0] = fmaxf(mx[0], p.x); mx[1] = fmaxf(mx[1], p.y); mx[2] = fmaxf(mx[2], p.z);
+        }
+        bbox_reduce(mn, mx);
+    }
+    // reduce per-thread boxes: warp shuffle, warp partials in smem, barrier, redundant final
+    __device__ void bbox_reduce(float* mn, float* mx) {
+        float* red = at<float>(L.red) + 8 * 2 * L.nwarps;   // after the 4 doubles per warp
+#pragma unroll
+        for (int k = 0; k < 3; k++) { mn[k] = wmin(mn[k]); mx[k] = wmax(mx[k]); }
+        if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < 3; k++) { red[6 * warp + k] = mn[k]; red[6 * warp + 3 + k] = mx[k]; }
+        }
+        __syncthreads();
+        float a[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, b[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+        for (int w = 0; w < L.nwarps; w++) {
+#pragma unroll
+            for (int k = 0; k < 3; k++) { a[k] = fminf(a[k], red[6 * w + k]); b[k] = fmaxf(b[k], red[6 * w + 3 + k]); }
+        }
+#pragma unroll
+        for (int k = 0; k < 3; k++) { bbmin[k] = a[k]; bbmax[k] = b[k]; }
+    }
+
+    // is image (ix,iy,iz) within the cutoff of the molecule's own box?
+    __device__ __forceinline__ bool image_active(int ix, int iy, int iz) const {
+        if (P.Rc2 <= 0.f) return true;
+        if (ix == 0 && iy == 0 && iz == 0) return true;
+        const float3 sh = image_shift(lv, ix, iy, iz);
+        // gap between [bbmin,bbmax] and [bbmin+sh, bbmax+sh] per axis
+        const float gx = fmaxf(0.f, fabsf(sh.x) - (bbmax[0] - bbmin[0]));
+        const float gy = fmaxf(0.f, fabsf(sh.y) - (bbmax[1] - bbmin[1]));
+        const float gz = fmaxf(0.f, fabsf(sh.z) - (bbmax[2] - bbmin[2]));
+        return gx * gx + gy * gy + gz * gz < P.Rc2;
+    }
+
+    // ------------------------------------------------------------------ phase 1
+    // returns this thread's energy contributions (only meaningful if ENERGY)
+    __device__ void forces(double& Eb, double& Enb, double& Eg) {
+        const int flags = P.flags;
+        const float4* spos = at<float4>(L.pos);
+        float4* fasm = at<float4>(L.fasm);
+        float4* fnb = at<float4>(L.fnb);
+        float4* fgr = at<float4>(L.fgrid);
+        const float4* sREQ = at<float4>(L.REQ);
+        const int4* sng = at<int4>(L.ng);
+        const int4* sngC = at<int4>(L.ngC);
+        float4* fng = at<float4>(L.fng);
+        // --- bonded (nodes); caps get a zero own-force
+        for (int ia = tid; ia < natoms; ia += T) {
+            if (ia >= nnode) { fasm[ia] = make_float4(0, 0, 0, 0); continue; }
+            BondedOut o;
+            eval_atom<ENERGY>(ia, natoms, nnode, flags, P.Fmax2NB, spos, sREQ, sng[ia], sngC[ia],
+                              at<float4>(L.apar)[ia], at<float4>(L.bL)[ia], at<float4>(L.bK)[ia],
+                              at<float4>(L.ksp)[ia], at<float4>(L.kpp)[ia], lv, P.npbc[0], P.npbc[1], P.npbc[2], o);
+            fasm[ia] = make_float4(o.fa.x, o.fa.y, o.fa.z, 0.f);
+            fasm[natoms + ia] = make_float4(o.fpi.x, o.fpi.y, o.fpi.z, 0.f);
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                fng[ia * 4 + k] = make_float4(o.fbs[k].x, o.fbs[k].y, o.fbs[k].z, 0.f);
+                fng[4 * L.maxNN + ia * 4 + k] = make_float4(o.fps[k].x, o.fps[k].y, o.fps[k].z, 0.f);
+            }
+            if (ENERGY) Eb += (double)o.E;
+        }
+        // --- non-bonded pairs: S lanes per atom i, j strided by S
+        if (flags & F_NONBONDED) {
+            const bool pbc = (flags & F_PBC) != 0;
+            const int npx = pbc ? P.npbc[0] : 0, npy = pbc ? P.npbc[1] : 0, npz = pbc ? P.npbc[2] : 0;
+            const int nxi = 2 * npx + 1, nyi = 2 * npy + 1;
+            const bool cut = P.Rc2 > 0.f;
+            const int nunits = natoms * S;
+            for (int u0 = 0; u0 < nunits; u0 += T) {
+                const int u = u0 + tid;
+                const int i = u / S, sub = u % S;
+                float fx = 0.f, fy = 0.f, fz = 0.f;
+                double e = 0.0;
+                if (i < natoms) {
+                    const float4 pi = spos[i];
+                    const float4 Ri = sREQ[i];
+                    const int4 ng = sng[i], ngC = sngC[i];
+                    for (int iz = -npz; iz <= npz; iz++)
+                        for (int iy = -npy; iy <= npy; iy++)
+                            for (int ix = -npx; ix <= npx; ix++) {
+                                if (!image_active(ix, iy, iz)) continue;
+                                const int ipbc = ((iz + npz) * nyi + (iy + npy)) * nxi + (ix + npx);
+                                const float3 sh = image_shift(lv, ix, iy, iz);
+                                const float pxs = pi.x - sh.x, pys = pi.y - sh.y, pzs = pi.z - sh.z;
+                                // excluded j for this image: self, and bonded neighbours whose cell is ipbc
+                                const int e0 = i;
+                                const int e1 = (ngC.x == ipbc || !pbc) ? ng.x : -1;
+                                const int e2 = (ngC.y == ipbc || !pbc) ? ng.y : -1;
+                                const int e3 = (ngC.z == ipbc || !pbc) ? ng.z : -1;
+                                const int e4 = (ngC.w == ipbc || !pbc) ? ng.w : -1;
+                                float ei = 0.f;
+                                for (int j = sub; j < natoms; j += S) {
+                                    const float4 pj = spos[j];
+                                    const float4 Rj = sREQ[j];
+                                    const float dx = pj.x - pxs, dy = pj.y - pys, dz = pj.z - pzs;
+                                    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                                    const bool ex = (j == e0) | (j == e1) | (j == e2) | (j == e3) | (j == e4);
+                                    if (ex) continue;
+                                    if (cut && r2 >= P.Rc2) continue;
+                                    if (COUNT) npair++;
+                                    const float R0 = Ri.x + Rj.x;
+                                    const float E0 = Ri.y * Rj.y;
+                                    const float Q = Ri.z * Rj.z;
+                                    const float hw = fminf(Ri.w * Rj.w, 0.f);
+                                    float eij = 0.f;
+                                    float F = ljqh<ENERGY>(r2, R0, E0, Q, hw, eij);
+                                    if (cut) {
+                                        // shifted-force Coulomb: F_el(r) - F_el(Rc) along r
+                                        const float ir = rsqrtf(r2);
+                                        F = fmaf(Q * P.kq_rc2, ir, F);
+                                        if (ENERGY) {
+                                            const float r = r2 * ir;
+                                            const float rc = sqrtf(1.f / P.kq_rc2);
+                                            eij += Q * P.kq_rc2 * (r - 2.f * rc);
+                                        }
+                                    }
+                                    fx = fmaf(dx, F, fx); fy = fmaf(dy, F, fy); fz = fmaf(dz, F, fz);
+                                    if (ENERGY) ei += eij;
+                                }
+                                if (ENERGY) e += (double)ei;
+                            }
+                }
+                // reduce over the S lanes of atom i
+#pragma unroll
+                for (int o = S / 2; o > 0; o >>= 1) {
+                    fx += __shfl_xor_sync(0xffffffffu, fx, o);
+                    fy += __shfl_xor_sync(0xffffffffu, fy, o);
+                    fz += __shfl_xor_sync(0xffffffffu, fz, o);
+                }
+                if (i < natoms && sub == 0) fnb[i] = make_float4(fx, fy, fz, 0.f);
+                if (ENERGY) Enb += 0.5 * e;
+            }
+        } else {
+            for (int a = tid; a < natoms; a += T) fnb[a] = make_float4(0, 0, 0, 0);
+        }
+        // --- GridFF B-spline: 4 lanes per atom (x-slices)
+        if (flags & F_GRID) {
+            const float4* sPLQ = at<float4>(L.PLQ);
+            const int nunits = natoms * 4;
+            for (int u0 = 0; u0 < nunits; u0 += T) {
+                const int u = u0 + tid;
+                const int i = u >> 2, a = u & 3;
+                float4 r = make_float4(0, 0, 0, 0);
+                if (i < natoms) {
+                    const float4 p = spos[i];
+                    const float3 uu = make_float3((p.x + gorg.x) * P.ginv[0], (p.y + gorg.y) * P.ginv[1],
+                                                  (p.z + gorg.z) * P.ginv[2]);
+                    r = grid_slice(P.grid, P.gn[0], P.gn[1], P.gn[2], uu, sPLQ[i], a);
+                }
+#pragma unroll
+                for (int o = 2; o > 0; o >>= 1) {
+                    r.x += __shfl_xor_sync(0xffffffffu, r.x, o);
+                    r.y += __shfl_xor_sync(0xffffffffu, r.y, o);
+                    r.z += __shfl_xor_sync(0xffffffffu, r.z, o);
+                    r.w += __shfl_xor_sync(0xffffffffu, r.w, o);
+                }
+                if (i < natoms && a == 0) {
+                    fgr[i] = make_float4(r.x * P.gmi[0], r.y * P.gmi[1], r.z * P.gmi[2], 0.f);
+                    if (ENERGY) Eg += (double)r.w;
+                }
+            }
+        } else {
+            for (int a = tid; a < natoms; a += T) fgr[a] = make_float4(0, 0, 0, 0);
+        }
+    }
+
+    // ------------------------------------------------------------------ phase 2
+    // assemble + clamp; FP64 partial sums of (vf, vv, ff) and max|f|^2 for this thread
+    __device__ void assemble(double& vf, double& vv, double& ff, float& fmax2, bool& bad) {
+        float4* fasm = at<float4>(L.fasm);
+        const float4* fnb = at<float4>(L.fnb);
+        const float4* fgr = at<float4>(L.fgrid);
+        const int4* sbk = at<int4>(L.bk);
+        const float4* fng = at<float4>(L.fng);
+        const float4* spos = at<float4>(L.pos);
+        const float4* svel = at<float4>(L.vel);
+        const float Fl2 = P.Flim * P.Flim;
+        for (int v = tid; v < nvecs; v += T) {
+            float3 f;
+            if (v < natoms) {
+                const float4 a = fasm[v], b = fnb[v], c = fgr[v];
+                f = make_float3(a.x + b.x + c.x, a.y + b.y + c.y, a.z + b.z + c.z);
+                const int4 bk = sbk[v];
+                const int bks[4] = {bk.x, bk.y, bk.z, bk.w};
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    if (bks[k] < 0) break;
+                    f = f + f3(fng[bks[k]]);
+                }
+            } else {
+                const int ia = v - natoms;
+                f = f3(fasm[v]);
+                const int4 bk = sbk[ia];
+                const int bks[4] = {bk.x, bk.y, bk.z, bk.w};
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    if (bks[k] < 0) break;
+                    f = f + f3(fng[4 * L.maxNN + bks[k]]);
+                }
+                const float3 u = f3(spos[v]);
+                f = fma3(u, -dot3(f, u), f);      // Vec3::makeOrthoU
+            }
+            if (P.Flim > 0.f) {
+                const float fr2 = dot3(f, f);
+                if (fr2 > Fl2) f = f * (P.Flim * rsqrtf(fr2));
+            }
+            fasm[v] = make_float4(f.x, f.y, f.z, 0.f);
+            const float4 vv4 = svel[v];
+            vf += (double)vv4.x * f.x + (double)vv4.y * f.y + (double)vv4.z * f.z;
+            vv += (double)vv4.x * vv4.x + (double)vv4.y * vv4.y + (double)vv4.z * vv4.z;
+            const double f2 = (double)f.x * f.x + (double)f.y * f.y + (double)f.z * f.z;
+            ff += f2;
+            fmax2 = fmaxf(fmax2, (float)f2);
+            bad |= !isfinite(f.x + f.y + f.z);
+        }
+    }
+
+    // block reduction of 3 doubles + one float max (+flag); result in all threads
+    __device__ void reduce4(double& a, double& b, double& c, float& m, bool& bad) {
+        double* red = at<double>(L.red);
+        a = wsum(a); b = wsum(b); c = wsum(c); m = wmax(m);
+        const int anybad = __any_sync(0xffffffffu, bad);
+        if (lane == 0) {
+            red[4 * warp + 0] = a; red[4 * warp + 1] = b; red[4 * warp + 2] = c;
+            reinterpret_cast<float*>(red + 4 * warp + 3)[0] = m;
+            reinterpret_cast<int*>(red + 4 * warp + 3)[1] = anybad;
+        }
+        __syncthreads();
+        a = 0; b = 0; c = 0; m = 0.f; int nb = 0;
+        for (int w = 0; w < L.nwarps; w++) {
+            a += red[4 * w + 0]; b += red[4 * w + 1]; c += red[4 * w + 2];
+            m = fmaxf(m, reinterpret_cast<const float*>(red + 4 * w + 3)[0]);
+            nb |= reinterpret_cast<const int*>(red + 4 * w + 3)[1];
+        }
+        bad = nb != 0;
+    }
+
+    // ------------------------------------------------------------------ phase 3
+    __device__ void move(double dt, double cv, double cfm, float* mn, float* mx) {
+        float4* spos = at<float4>(L.pos);
+        float4* svel = at<float4>(L.vel);
+        const float4* fasm = at<float4>(L.fasm);
+        const float dtf = (float)dt;
+        const float cvf = (float)cv;
+        const float kf = (float)((double)dtf + cfm);
+        for (int v = tid; v < nvecs; v += T) {
+            float3 f = f3(fasm[v]), ve = f3(svel[v]), p = f3(spos[v]);
+            const bool bPi = v >= natoms;
+            if (bPi) f = fma3(p, -dot3(p, f), f);
+            ve = ve * cvf;
+            ve = fma3(f, kf, ve);
+            if (bPi) ve = fma3(p, -dot3(p, ve), ve);
+            p = fma3(ve, dtf, p);
+            if (bPi) p = p * rsqrtf(dot3(p, p));
+            spos[v] = make_float4(p.x, p.y, p.z, 0.f);
+            svel[v] = make_float4(ve.x, ve.y, ve.z, 0.f);
+            if (!bPi) {
+                mn[0] = fminf(mn[0], p.x); mn[1] = fminf(mn[1], p.y); mn[2] = fminf(mn[2], p.z);
+                mx[0] = fmaxf(mx[0], p.x); mx[1] = fmaxf(mx[1], p.y); mx[2] = fmaxf(mx[2], p.z);
+            }
+        }
+    }
+
+    __device__ void store_state(int status, int steps, float fconv, double dt, double damping, int lastNeg, double total) {
+        const float4* spos = at<float4>(L.pos);
+        const float4* svel = at<float4>(L.vel);
+        const float4* fasm = at<float4>(L.fasm);
+        for (int v = tid; v < nvecs; v += T) {
+            Y.pos[voff + v] = spos[v];
+            Y.vel[voff + v] = svel[v];
+            Y.force[voff + v] = fasm[v];
+        }
+        if (tid == 0) {
+            Y.fire[isys] = make_double4(dt, damping, (double)lastNeg, total);
+            Y.status[isys] = status;
+            Y.nsteps[isys] = steps;
+            Y.fconv[isys] = fconv;
+        }
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Persistent relaxation: claims systems from queue[] via counter.
+template <int T, int S, bool COUNT>
+__global__ void __launch_bounds__(T) relax_kernel(Params P, Systems Y, const int* __restrict__ queue, int nqueue,
+                                                  int* counter, int maxNA, int maxNN) {
+    extern __shared__ __align__(16) char smem[];
+    __shared__ int s_claim;
+    const SmemLayout L = smem_layout(maxNA, maxNN, T);
+    Engine<T, S, false, COUNT> E(P, Y, smem, L);
+    while (true) {
+        if (threadIdx.x == 0) s_claim = atomicAdd(counter, 1);
+        __syncthreads();
+        const int q = s_claim;
+        if (q >= nqueue) break;
+        const int s = queue[q];
+        E.load(s);
+        const double4 fs = Y.fire[s];
+        double dt = fs.x, damping = fs.y, total = fs.w;
+        int lastNeg = (int)fs.z;
+        __syncthreads();
+        E.bbox_from_smem();
+        int status = ST_MAXSTEPS, itr = 0;
+        float meas = 0.f;
+        for (itr = 0; itr < P.nstep_max; itr++) {
+            double d0 = 0, d1 = 0, d2 = 0;
+            E.forces(d0, d1, d2);
+            __syncthreads();
+            double vf = 0, vv = 0, ff = 0;
+            float fmax2 = 0.f;
+            bool bad = false;
+            E.assemble(vf, vv, ff, fmax2, bad);
+            E.reduce4(vf, vv, ff, fmax2, bad);
+            if (bad) { status = ST_NAN; break; }
+            // DynamicOpt::FIRE_update_params (FP64, identical in every thread)
+            const double f_len = sqrt(ff), v_len = sqrt(vv);
+            const double cos_vf = vf / (f_len * v_len + 1e-32);
+            const double renorm_vf = v_len / (f_len + 1e-32);
+            double cv, cf;
+            if (cos_vf < 0.0) { cv = P.cv_kill; cf = 0.0; } else { cv = 1.0 - damping; cf = damping; }
+            cf = renorm_vf * cf;
+            if (cos_vf < 0.0) {
+                dt = fmax(dt * P.fdec, P.dt_min);
+                lastNeg = 0;
+                damping = P.damp_max;
+            } else {
+                if (lastNeg > P.minLastNeg) { dt = fmin(dt * P.finc, P.dt_max); damping = damping * P.falpha; }
+                lastNeg++;
+            }
+            float mn[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, mx[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+            E.move(dt, cv, renorm_vf * cf, mn, mx);
+            total += 1.0;
+            const double m = (P.conv_mode == 0) ? ff : (double)fmax2;
+            meas = (float)sqrt(m);
+            if (m < P.Fconv2) { status = ST_CONVERGED; itr++; E.bbox_reduce(mn, mx); break; }
+            E.bbox_reduce(mn, mx);   // contains the end-of-step barrier
+        }
+        // converged at step itr-1 (reference returns the loop index at break)
+        const int steps = (status == ST_CONVERGED) ? itr - 1 : itr;
+        __syncthreads();
+        E.store_state(status, steps, meas, dt, damping, lastNeg, total);
+        if (COUNT) {
+            // force evaluations done for this system: itr loop iterations
+            if (threadIdx.x == 0) {
+                atomicAdd(Y.counters + 1, (unsigned long long)itr * (unsigned long long)E.natoms);
+                atomicAdd(Y.counters + 2, (unsigned long long)itr);
+            }
+        }
+        __syncthreads();
+    }
+    if (COUNT) atomicAdd(Y.counters, E.npair);
+}
+
+// One force (and energy) evaluation per system; blockIdx.x indexes queue[].
+template <int T, int S, bool ENERGY>
+__global__ void __launch_bounds__(T) eval_kernel(Params P, Systems Y, const int* __restrict__ queue, int nqueue,
+                                                 int maxNA, int maxNN) {
+    extern __shared__ __align__(16) char smem[];
+    const SmemLayout L = smem_layout(maxNA, maxNN, T);
+    Engine<T, S, ENERGY> E(P, Y, smem, L);
+    const int q = blockIdx.x;
+    if (q >= nqueue) return;
+    const int s = queue[q];
+    E.load(s);
+    __syncthreads();
+    E.bbox_from_smem();
+    double Eb = 0, Enb = 0, Eg = 0;
+    E.forces(Eb, Enb, Eg);
+    __syncthreads();
+    // (the host passes Flim <= 0 here: eval reports unclamped forces)
+    double vf = 0, vv = 0, ff = 0;
+    float fmax2 = 0.f;
+    bool bad = false;
+    E.assemble(vf, vv, ff, fmax2, bad);
+    __syncthreads();
+    const float4* fasm = E.template at<float4>(L.fasm);
+    for (int v = threadIdx.x; v < E.nvecs; v += T) Y.force[E.voff + v] = fasm[v];
+    if (ENERGY) {
+        double eb = Eb, enb = Enb, eg = Eg;
+        float dummy = 0.f;
+        bool b2 = false;
+        __syncthreads();
+        E.reduce4(eb, enb, eg, dummy, b2);
+        if (threadIdx.x == 0) Y.energy[s] = make_double4(eb, enb, eg, eb + enb + eg);
+    }
+    if (threadIdx.x == 0) Y.fconv[s] = sqrtf(fmax2);
+}
+
+// B-spline sample of n points (grid parity tests): fe = (Fx, Fy, Fz, E)
+__global__ void grid_sample_kernel(Params P, int n, const float4* __restrict__ pos, const float4* __restrict__ PLQ,
+                                   float4* __restrict__ fe) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = u >> 2, a = u & 3;
+    float4 r = make_float4(0, 0, 0, 0);
+    if (i < n) {
+        const float4 p = pos[i];
+        const float3 uu = make_float3(p.x * P.ginv[0], p.y * P.ginv[1], p.z * P.ginv[2]);
+        r = grid_slice(P.grid, P.gn[0], P.gn[1], P.gn[2], uu, PLQ[i], a);
+    }
+#pragma unroll
+    for (int o = 2; o > 0; o >>= 1) {
+        r.x += __shfl_xor_sync(0xffffffffu, r.x, o);
+        r.y += __shfl_xor_sync(0xffffffffu, r.y, o);
+        r.z += __shfl_xor_sync(0xffffffffu, r.z, o);
+        r.w += __shfl_xor_sync(0xffffffffu, r.w, o);
+    }
+    if (i < n && a == 0) fe[i] = make_float4(r.x * P.gmi[0], r.y * P.gmi[1], r.z * P.gmi[2], r.w);
+}
+
+
+// address of the kernel instantiation for (T, S)
+#define MMFF_TS_SWITCH(T, S, ...)                                                            \
+    switch (T * 16 + S) {                                                                     \
+        case 64 * 16 + 1: { constexpr int T_ = 64, S_ = 1; __VA_ARGS__; }                            \
+        case 64 * 16 + 2: { constexpr int T_ = 64, S_ = 2; __VA_ARGS__; }                            \
+        case 64 * 16 + 4: { constexpr int T_ = 64, S_ = 4; __VA_ARGS__; }                            \
+        case 64 * 16 + 8: { constexpr int T_ = 64, S_ = 8; __VA_ARGS__; }                            \
+        case 128 * 16 + 1: { constexpr int T_ = 128, S_ = 1; __VA_ARGS__; }                          \
+        case 128 * 16 + 2: { constexpr int T_ = 128, S_ = 2; __VA_ARGS__; }                          \
+        case 128 * 16 + 4: { constexpr int T_ = 128, S_ = 4; __VA_ARGS__; }                          \
+        case 128 * 16 + 8: { constexpr int T_ = 128, S_ = 8; __VA_ARGS__; }                          \
+        case 256 * 16 + 1: { constexpr int T_ = 256, S_ = 1; __VA_ARGS__; }                          \
+        case 256 * 16 + 2: { constexpr int T_ = 256, S_ = 2; __VA_ARGS__; }                          \
+        case 256 * 16 + 4: { constexpr int T_ = 256, S_ = 4; __VA_ARGS__; }                          \
+        case 256 * 16 + 8: { constexpr int T_ = 256, S_ = 8; __VA_ARGS__; }                          \
+        case 512 * 16 + 1: { constexpr int T_ = 512, S_ = 1; __VA_ARGS__; }                          \
+        case 512 * 16 + 2: { constexpr int T_ = 512, S_ = 2; __VA_ARGS__; }                          \
+        case 512 * 16 + 4: { constexpr int T_ = 512, S_ = 4; __VA_ARGS__; }                          \
+        case 512 * 16 + 8: { constexpr int T_ = 512, S_ = 8; __VA_ARGS__; }                          \
+        default: return nullptr;                                                              \
+    }
+
+void* relax_fn(int T, int S, bool count) {
+    if (count) { MMFF_TS_SWITCH(T, S, return (void*)relax_kernel<T_, S_, true>) }
+    MMFF_TS_SWITCH(T, S, return (void*)relax_kernel<T_, S_, false>)
+}
+void* eval_fn(int T, int S, bool energy) {
+    if (energy) { MMFF_TS_SWITCH(T, S, return (void*)eval_kernel<T_, S_, true>) }
+    MMFF_TS_SWITCH(T, S, return (void*)eval_kernel<T_, S_, false>)
+}
+
+}  // namespace mmff

@@ -1,0 +1,594 @@
+// mmff_world.cu -- device-resident world of many MMFF systems and the C-ABI
+// that drives it (declared in include/MMFFmulti_lib.h).
+//
+// The host side packs systems of uneven size back to back (CSR offsets), moves
+// each system into a local frame (positions relative to its own centroid, so
+// FP32 coordinates keep ~5e-7 A resolution), converts the force-field
+// parameters to the FP32 layout the kernels read, groups systems into size
+// buckets and launches one persistent relaxation kernel per bucket.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "MMFFmulti_lib.h"
+#include "mmff_device.cuh"
+
+namespace mmff {
+// kernels (mmff_relax.cu, mmff_grid.cu)
+template <int T, int S, bool C> __global__ void relax_kernel(Params, Systems, const int*, int, int*, int, int);
+template <int T, int S, bool E> __global__ void eval_kernel(Params, Systems, const int*, int, int, int);
+__global__ void grid_sample_kernel(Params, int, const float4*, const float4*, float4*);
+__global__ void grid_potential_kernel(int, int, int, double3, double3, int, const double4*, const double2*,
+                                      const double3*, int, const double3*, int, double, double*);
+__global__ void solve_open_kernel(double*, long, int, long, long, int, long, double*);
+__global__ void solve_periodic_kernel(double*, long, int, long, long, int, long, double*);
+__global__ void pack_grid_kernel(long, const double*, float4*);
+void* relax_fn(int T, int S, bool count);
+void* eval_fn(int T, int S, bool energy);
+}  // namespace mmff
+
+using namespace mmff;
+
+namespace {
+
+std::string g_err;
+int fail(const char* fmt, ...) {
+    char buf[512];
+    va_list ap; va_start(ap, fmt); vsnprintf(buf, sizeof buf, fmt, ap); va_end(ap);
+    g_err = buf;
+    return -1;
+}
+#define CK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) return fail("%s: %s (%s:%d)", #x, cudaGetErrorString(e_), __FILE__, __LINE__); } while (0)
+
+template <class X> struct DBuf {
+    X* p = nullptr; size_t n = 0;
+    int ensure(size_t cnt) {
+        if (cnt <= n && p) return 0;
+        if (p) cudaFree(p);
+        p = nullptr; n = 0;
+        if (cnt == 0) return 0;
+        cudaError_t e = cudaMalloc(&p, cnt * sizeof(X));
+        if (e != cudaSuccess) return fail("cudaMalloc(%zu B): %s", cnt * sizeof(X), cudaGetErrorString(e));
+        n = cnt;
+        return 0;
+    }
+    void release() { if (p) cudaFree(p); p = nullptr; n = 0; }
+};
+
+struct Bucket {
+    int T = 64, S = 1, maxNA = 0, maxNN = 0;
+    std::vector<int> sys;          // system indices, largest first
+    DBuf<int> queue;
+    int smem = 0, grid = 0;
+};
+
+struct World {
+    bool ready = false;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<cudaStream_t> bstreams;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evfork = nullptr;
+    std::vector<cudaEvent_t> bev;
+    // grid
+    DBuf<float4> grid;
+    int gn[3] = {0, 0, 0};
+    double gpos0[3] = {0, 0, 0}, gstep[3] = {1, 1, 1};
+    // systems
+    int nsys = 0, NA = 0, NN = 0, NV = 0;
+    std::vector<int> natoms, nnode;
+    std::vector<int4> desc;
+    std::vector<double> orig;      // [nsys*3]
+    DBuf<int4> d_desc; DBuf<int> d_nnode; DBuf<float> d_lvec; DBuf<float4> d_gorg;
+    DBuf<float4> d_REQ, d_PLQ; DBuf<int4> d_ng, d_ngC, d_bk;
+    DBuf<float4> d_apar, d_bL, d_bK, d_ksp, d_kpp;
+    DBuf<float4> d_pos, d_vel, d_force, d_pos0, d_vel0;
+    DBuf<double4> d_fire, d_fire0, d_energy;
+    DBuf<int> d_status, d_nsteps, d_counter;
+    DBuf<unsigned long long> d_stats;
+    bool count = false;
+    DBuf<float> d_fconv;
+    // parameters
+    int flags = F_BONDS | F_PIPI | F_PISIGMA | F_ANGLES | F_SUB_ANGLE_NB | F_NONBONDED | F_GRID | F_PBC;
+    int npbc[3] = {1, 1, 0};
+    double Rcut = -1.0, alphaMorse = 1.5, FmaxNB = 10.0;
+    double fire[9] = {0.1, 0.01, 0.1, 1.1, 0.5, 0.8, 3, 0.0, -1.0};  // dt_max dt_min damp_max finc fdec falpha minLastNeg cv_kill Flim
+    // launch configuration (0 = heuristic)
+    int force_T = 0, force_S = 0;
+    std::vector<Bucket> buckets;
+    bool buckets_dirty = true;
+};
+
+World W;
+
+int ensure_ready() {
+    if (W.ready) return 0;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) return fail("no CUDA device available (%s)", cudaGetErrorString(e));
+    CK(cudaSetDevice(W.device));
+    CK(cudaStreamCreateWithFlags(&W.stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&W.ev0));
+    CK(cudaEventCreate(&W.ev1));
+    CK(cudaEventCreateWithFlags(&W.evfork, cudaEventDisableTiming));
+    W.ready = true;
+    return 0;
+}
+
+Params make_params(bool for_eval, int nstep_max, double Fconv, int conv_mode) {
+    Params P;
+    memset(&P, 0, sizeof P);
+    P.flags = W.flags;
+    if (!W.grid.p) P.flags &= ~F_GRID;
+    for (int k = 0; k < 3; k++) P.npbc[k] = W.npbc[k];
+    P.Rc2 = W.Rcut > 0 ? (float)(W.Rcut * W.Rcut) : 0.f;
+    P.kq_rc2 = W.Rcut > 0 ? (float)(1.0 / (W.Rcut * W.Rcut)) : 0.f;
+    P.Fmax2NB = (float)(W.FmaxNB * W.FmaxNB);
+    for (int k = 0; k < 3; k++) {
+        P.gn[k] = W.gn[k];
+        P.ginv[k] = (float)(1.0 / W.gstep[k]);
+        P.gmi[k] = (float)(-1.0 / W.gstep[k]);
+    }
+    P.grid = W.grid.p;
+    P.dt_max = W.fire[0]; P.dt_min = W.fire[1]; P.damp_max = W.fire[2]; P.finc = W.fire[3];
+    P.fdec = W.fire[4]; P.falpha = W.fire[5]; P.minLastNeg = (int)W.fire[6]; P.cv_kill = W.fire[7];
+    P.Flim = for_eval ? -1.f : (float)W.fire[8];
+    P.Fconv2 = Fconv * Fconv;
+    P.conv_mode = conv_mode;
+    P.nstep_max = nstep_max;
+    return P;
+}
+
+Systems make_systems() {
+    Systems Y;
+    Y.nsys = W.nsys;
+    Y.desc = W.d_desc.p; Y.nnode = W.d_nnode.p; Y.lvec = W.d_lvec.p; Y.gorg = W.d_gorg.p;
+    Y.REQ = W.d_REQ.p; Y.PLQ = W.d_PLQ.p; Y.neighs = W.d_ng.p; Y.neighCell = W.d_ngC.p; Y.bkneighs = W.d_bk.p;
+    Y.apars = W.d_apar.p; Y.bLs = W.d_bL.p; Y.bKs = W.d_bK.p; Y.Ksp = W.d_ksp.p; Y.Kpp = W.d_kpp.p;
+    Y.pos = W.d_pos.p; Y.vel = W.d_vel.p; Y.force = W.d_force.p; Y.fire = W.d_fire.p;
+    Y.status = W.d_status.p; Y.nsteps = W.d_nsteps.p; Y.fconv = W.d_fconv.p; Y.energy = W.d_energy.p;
+    Y.counters = W.d_stats.p;
+    return Y;
+}
+
+int pow2_floor(int x) { int p = 1; while (p * 2 <= x) p *= 2; return p; }
+
+// size buckets: thread count T >= atoms (<= 512); S lanes per atom in the pair sum
+int build_buckets() {
+    W.buckets.clear();
+    const int Ts[4] = {64, 128, 256, 512};
+    std::vector<std::vector<int>> groups(4);
+    for (int s = 0; s < W.nsys; s++) {
+        int na = W.natoms[s], b = 3;
+        for (int k = 0; k < 4; k++) if (na <= Ts[k]) { b = k; break; }
+        if (W.force_T) { for (int k = 0; k < 4; k++) if (Ts[k] == W.force_T) b = k; }
+        groups[b].push_back(s);
+    }
+    int dev_smem = 0;
+    CK(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, W.device));
+    int nsm = 0;
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, W.device));
+    for (int k = 3; k >= 0; k--) {
+        if (groups[k].empty()) continue;
+        Bucket B;
+        B.T = Ts[k];
+        B.sys = groups[k];
+        std::stable_sort(B.sys.begin(), B.sys.end(), [](int a, int b) { return W.natoms[a] > W.natoms[b]; });
+        for (int s : B.sys) { B.maxNA = std::max(B.maxNA, W.natoms[s]); B.maxNN = std::max(B.maxNN, W.nnode[s]); }
+        int S = pow2_floor(std::max(1, B.T / std::max(1, B.maxNA)));
+        B.S = std::min(S, 8);
+        if (W.force_S) B.S = W.force_S;
+        B.smem = smem_layout(B.maxNA, B.maxNN, B.T).total;
+        if (B.smem > dev_smem) return fail("system too large for shared memory: %d B > %d B", B.smem, dev_smem);
+        void* fn = relax_fn(B.T, B.S, false);
+        if (!fn) return fail("no kernel for T=%d S=%d", B.T, B.S);
+        CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, B.smem));
+        CK(cudaFuncSetAttribute(relax_fn(B.T, B.S, true), cudaFuncAttributeMaxDynamicSharedMemorySize, B.smem));
+        for (int e = 0; e < 2; e++) CK(cudaFuncSetAttribute(eval_fn(B.T, B.S, e), cudaFuncAttributeMaxDynamicSharedMemorySize, B.smem));
+        int occ = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, B.T, B.smem));
+        if (occ < 1) return fail("kernel cannot be resident (T=%d smem=%d)", B.T, B.smem);
+        B.grid = std::min((int)B.sys.size(), occ * nsm);
+        if (B.queue.ensure(B.sys.size())) return -1;
+        CK(cudaMemcpy(B.queue.p, B.sys.data(), B.sys.size() * sizeof(int), cudaMemcpyHostToDevice));
+        W.buckets.push_back(std::move(B));
+    }
+    while (W.bstreams.size() < W.buckets.size()) {
+        cudaStream_t s; CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); W.bstreams.push_back(s);
+        cudaEvent_t e; CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming)); W.bev.push_back(e);
+    }
+    W.buckets_dirty = false;
+    return 0;
+}
+
+template <class X> int upload(DBuf<X>& d, const std::vector<X>& h) {
+    if (d.ensure(h.size())) return -1;
+    if (!h.empty()) CK(cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(X), cudaMemcpyHostToDevice, W.stream));
+    return 0;
+}
+
+}  // namespace
+
+// ============================================================================ C-ABI
+extern "C" {
+
+const char* mmff_last_error(void) { return g_err.c_str(); }
+
+int mmff_init_device(int device) {
+    if (W.ready && W.device == device) return 0;
+    W.device = device;
+    W.ready = false;
+    return ensure_ready();
+}
+
+int mmff_sync(void) {
+    if (ensure_ready()) return -1;
+    CK(cudaStreamSynchronize(W.stream));
+    CK(cudaGetLastError());
+    return 0;
+}
+
+int mmff_set_params(int flags, const int* nPBC, double Rcut, double alphaMorse, double FmaxNonBonded) {
+    W.flags = flags;
+    if (nPBC) for (int k = 0; k < 3; k++) W.npbc[k] = nPBC[k];
+    W.Rcut = Rcut;
+    W.alphaMorse = alphaMorse;
+    W.FmaxNB = FmaxNonBonded;
+    return 0;
+}
+
+int mmff_set_fire(double dt_max, double dt_min, double damp_max, double finc, double fdec, double falpha,
+                  int minLastNeg, double cv_kill, double Flim) {
+    double f[9] = {dt_max, dt_min, damp_max, finc, fdec, falpha, (double)minLastNeg, cv_kill, Flim};
+    memcpy(W.fire, f, sizeof f);
+    return 0;
+}
+
+int mmff_set_launch(int threads, int pair_split) {
+    if (threads && threads != 64 && threads != 128 && threads != 256 && threads != 512) return fail("threads must be 64/128/256/512");
+    if (pair_split && pair_split != 1 && pair_split != 2 && pair_split != 4 && pair_split != 8) return fail("pair_split must be 1/2/4/8");
+    W.force_T = threads; W.force_S = pair_split; W.buckets_dirty = true;
+    return 0;
+}
+
+int mmff_grid_upload(int nx, int ny, int nz, const double* pos0, const double* step, const double* coefs) {
+    if (ensure_ready()) return -1;
+    if (nx < 4 || ny < 4 || nz < 8) return fail("grid too small (%d,%d,%d)", nx, ny, nz);
+    const size_t n = (size_t)nx * ny * nz;
+    std::vector<float4> h(n);
+    for (size_t i = 0; i < n; i++) h[i] = make_float4((float)coefs[3 * i], (float)coefs[3 * i + 1], (float)coefs[3 * i + 2], 0.f);
+    if (W.grid.ensure(n)) return -1;
+    CK(cudaMemcpyAsync(W.grid.p, h.data(), n * sizeof(float4), cudaMemcpyHostToDevice, W.stream));
+    CK(cudaStreamSynchronize(W.stream));
+    W.gn[0] = nx; W.gn[1] = ny; W.gn[2] = nz;
+    for (int k = 0; k < 3; k++) { W.gpos0[k] = pos0[k]; W.gstep[k] = step[k]; }
+    return 0;
+}
+
+int mmff_grid_build(int nsub, const double* spos, const double* sREQ, const double* lvec, const int* nPBC_mors,
+                    const int* nPBC_coul, double alphaMorse, int nx, int ny, int nz, const double* pos0,
+                    const double* step, double* coefs_out) {
+    if (ensure_ready()) return -1;
+    if (nx < 4 || ny < 4 || nz < 8 || nsub < 1) return fail("bad grid build arguments");
+    const long ntot = (long)nx * ny * nz;
+    std::vector<double4> hq(nsub);
+    std::vector<double2> hr(nsub);
+    for (int i = 0; i < nsub; i++) {
+        hq[i] = make_double4(spos[3 * i], spos[3 * i + 1], spos[3 * i + 2], sREQ[4 * i + 2]);
+        hr[i] = make_double2(sREQ[4 * i], sREQ[4 * i + 1]);
+    }
+    auto shifts = [&](const int* np) {
+        std::vector<double3> s;
+        for (int iz = -np[2]; iz <= np[2]; iz++) for (int iy = -np[1]; iy <= np[1]; iy++) for (int ix = -np[0]; ix <= np[0]; ix++)
+            s.push_back(make_double3(lvec[0] * ix + lvec[3] * iy + lvec[6] * iz, lvec[1] * ix + lvec[4] * iy + lvec[7] * iz,
+                                     lvec[2] * ix + lvec[5] * iy + lvec[8] * iz));
+        return s;
+    };
+    std::vector<double3> sm = shifts(nPBC_mors), sc = shifts(nPBC_coul);
+    DBuf<double4> dq; DBuf<double2> dr; DBuf<double3> dsm, dsc; DBuf<double> V, work;
+    if (dq.ensure(nsub) || dr.ensure(nsub) || dsm.ensure(sm.size()) || dsc.ensure(sc.size()) || V.ensure(3 * ntot)) return -1;
+    CK(cudaMemcpy(dq.p, hq.data(), nsub * sizeof(double4), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dr.p, hr.data(), nsub * sizeof(double2), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dsm.p, sm.data(), sm.size() * sizeof(double3), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dsc.p, sc.data(), sc.size() * sizeof(double3), cudaMemcpyHostToDevice));
+    const int tb = 128;
+    grid_potential_kernel<<<(unsigned)((ntot + tb - 1) / tb), tb, 0, W.stream>>>(
+        nx, ny, nz, make_double3(pos0[0], pos0[1], pos0[2]), make_double3(step[0], step[1], step[2]), nsub, dq.p, dr.p,
+        dsm.p, (int)sm.size(), dsc.p, (int)sc.size(), alphaMorse, V.p);
+    CK(cudaGetLastError());
+    // z lines (open), then y and x (periodic)
+    const long lz = (long)nx * ny, ly = (long)nx * nz, lx = (long)ny * nz;
+    const long wmax = std::max(lz * nz, std::max(ly * 2 * ny, lx * 2 * nx));
+    if (work.ensure(wmax)) return -1;
+    solve_open_kernel<<<(unsigned)((lz + 127) / 128), 128, 0, W.stream>>>(V.p, lz, nz, nz, 1, 1, 0, work.p);
+    solve_periodic_kernel<<<(unsigned)((ly + 127) / 128), 128, 0, W.stream>>>(V.p, ly, ny, (long)ny * nz, nz, nz, 1, work.p);
+    solve_periodic_kernel<<<(unsigned)((lx + 127) / 128), 128, 0, W.stream>>>(V.p, lx, nx, 1, (long)ny * nz, 1, 0, work.p);
+    CK(cudaGetLastError());
+    if (W.grid.ensure(ntot)) return -1;
+    pack_grid_kernel<<<(unsigned)((ntot + 255) / 256), 256, 0, W.stream>>>(ntot, V.p, W.grid.p);
+    CK(cudaGetLastError());
+    if (coefs_out) CK(cudaMemcpyAsync(coefs_out, V.p, 3 * ntot * sizeof(double), cudaMemcpyDeviceToHost, W.stream));
+    CK(cudaStreamSynchronize(W.stream));
+    W.gn[0] = nx; W.gn[1] = ny; W.gn[2] = nz;
+    for (int k = 0; k < 3; k++) { W.gpos0[k] = pos0[k]; W.gstep[k] = step[k]; }
+    work.release(); V.release(); dq.release(); dr.release(); dsm.release(); dsc.release();
+    return 0;
+}
+
+int mmff_systems_upload(int nsys, const int* natoms, const int* nnode, const double* pos, const double* vel,
+                        const int* neighs, const int* neighCell, const int* bkneighs, const double* REQs,
+                        const double* apars, const double* bLs, const double* bKs, const double* Ksp,
+                        const double* Kpp, const double* lvec) {
+    if (ensure_ready()) return -1;
+    if (nsys < 1) return fail("nsys must be >= 1");
+    W.nsys = nsys;
+    W.natoms.assign(natoms, natoms + nsys);
+    W.nnode.assign(nnode, nnode + nsys);
+    W.desc.resize(nsys);
+    int NA = 0, NN = 0, NV = 0;
+    for (int s = 0; s < nsys; s++) {
+        if (natoms[s] < 1 || nnode[s] < 0 || nnode[s] > natoms[s]) return fail("system %d: bad sizes natoms=%d nnode=%d", s, natoms[s], nnode[s]);
+        W.desc[s] = make_int4(NA, NN, NV, natoms[s]);
+        NA += natoms[s]; NN += nnode[s]; NV += natoms[s] + nnode[s];
+    }
+    W.NA = NA; W.NN = NN; W.NV = NV;
+    // validate topology indices (never hand the kernels an out-of-range index)
+    const int np = (2 * W.npbc[0] + 1) * (2 * W.npbc[1] + 1) * (2 * W.npbc[2] + 1);
+    for (int s = 0; s < nsys; s++) {
+        const int a0 = W.desc[s].x, na = natoms[s], nn = nnode[s];
+        for (int i = 0; i < na; i++) for (int k = 0; k < 4; k++) {
+            const int j = neighs[4 * (a0 + i) + k], c = neighCell[4 * (a0 + i) + k], b = bkneighs[4 * (a0 + i) + k];
+            if (j >= na || j < -1) return fail("system %d atom %d: neighbour %d out of range", s, i, j);
+            if (j >= 0 && i < nn && (c < 0 || c >= np) && (W.flags & F_PBC)) return fail("system %d atom %d: neighCell %d out of range", s, i, c);
+            if (b >= 4 * nn || b < -1) return fail("system %d atom %d: bkneigh %d out of range", s, i, b);
+        }
+    }
+    W.orig.assign(3 * nsys, 0.0);
+    std::vector<float4> hpos(NV), hvel(NV), hREQ(NA), hPLQ(NA), hap(NN), hbL(NN), hbK(NN), hks(NN), hkp(NN), hgorg(nsys);
+    std::vector<int4> hng(NA), hngC(NA), hbk(NA);
+    std::vector<float> hlv(9 * nsys);
+    std::vector<double4> hfire(nsys);
+    const double sqk = std::sqrt(14.3996448915);
+    for (int s = 0; s < nsys; s++) {
+        const int a0 = W.desc[s].x, n0 = W.desc[s].y, v0 = W.desc[s].z, na = natoms[s], nn = nnode[s];
+        double c[3] = {0, 0, 0};
+        for (int i = 0; i < na; i++) for (int k = 0; k < 3; k++) c[k] += pos[3 * (v0 + i) + k];
+        for (int k = 0; k < 3; k++) { c[k] /= na; W.orig[3 * s + k] = c[k]; }
+        for (int i = 0; i < na + nn; i++) {
+            const double* p = pos + 3 * (v0 + i);
+            if (i < na) hpos[v0 + i] = make_float4((float)(p[0] - c[0]), (float)(p[1] - c[1]), (float)(p[2] - c[2]), 0.f);
+            else        hpos[v0 + i] = make_float4((float)p[0], (float)p[1], (float)p[2], 0.f);
+            const double* v = vel ? vel + 3 * (v0 + i) : nullptr;
+            hvel[v0 + i] = v ? make_float4((float)v[0], (float)v[1], (float)v[2], 0.f) : make_float4(0, 0, 0, 0);
+        }
+        for (int i = 0; i < na; i++) {
+            const double* R = REQs + 4 * (a0 + i);
+            hREQ[a0 + i] = make_float4((float)R[0], (float)R[1], (float)(R[2] * sqk), (float)R[3]);
+            // Forces.h:611 REQ2PLQ_d
+            const double e = std::exp(W.alphaMorse * R[0]);
+            const double cL = e * R[1], cP = e * cL;
+            hPLQ[a0 + i] = make_float4((float)cP, (float)cL, (float)R[2], (float)(e * e * R[3]));
+            const int* g = neighs + 4 * (a0 + i); hng[a0 + i] = make_int4(g[0], g[1], g[2], g[3]);
+            const int* gc = neighCell + 4 * (a0 + i); hngC[a0 + i] = make_int4(gc[0], gc[1], gc[2], gc[3]);
+            const int* b = bkneighs + 4 * (a0 + i); hbk[a0 + i] = make_int4(b[0], b[1], b[2], b[3]);
+        }
+        for (int i = 0; i < nn; i++) {
+            auto f4 = [&](const double* a) { return make_float4((float)a[4 * (n0 + i)], (float)a[4 * (n0 + i) + 1], (float)a[4 * (n0 + i) + 2], (float)a[4 * (n0 + i) + 3]); };
+            hap[n0 + i] = f4(apars); hbL[n0 + i] = f4(bLs); hbK[n0 + i] = f4(bKs); hks[n0 + i] = f4(Ksp); hkp[n0 + i] = f4(Kpp);
+        }
+        for (int k = 0; k < 9; k++) hlv[9 * s + k] = (float)lvec[9 * s + k];
+        hgorg[s] = make_float4((float)(c[0] - W.gpos0[0]), (float)(c[1] - W.gpos0[1]), (float)(c[2] - W.gpos0[2]), 0.f);
+        hfire[s] = make_double4(W.fire[0], W.fire[2], 0.0, 0.0);
+    }
+    std::vector<int4> hdesc = W.desc;
+    if (upload(W.d_desc, hdesc) || upload(W.d_nnode, W.nnode) || upload(W.d_lvec, hlv) || upload(W.d_gorg, hgorg) ||
+        upload(W.d_REQ, hREQ) || upload(W.d_PLQ, hPLQ) || upload(W.d_ng, hng) || upload(W.d_ngC, hngC) ||
+        upload(W.d_bk, hbk) || upload(W.d_apar, hap) || upload(W.d_bL, hbL) || upload(W.d_bK, hbK) ||
+        upload(W.d_ksp, hks) || upload(W.d_kpp, hkp) || upload(W.d_pos, hpos) || upload(W.d_vel, hvel) ||
+        upload(W.d_pos0, hpos) || upload(W.d_vel0, hvel) || upload(W.d_fire, hfire) || upload(W.d_fire0, hfire))
+        return -1;
+    if (W.d_force.ensure(NV) || W.d_energy.ensure(nsys) || W.d_status.ensure(nsys) || W.d_nsteps.ensure(nsys) ||
+        W.d_fconv.ensure(nsys) || W.d_counter.ensure(64) || W.d_stats.ensure(8))
+        return -1;
+    CK(cudaMemsetAsync(W.d_status.p, 0, nsys * sizeof(int), W.stream));
+    CK(cudaMemsetAsync(W.d_nsteps.p, 0, nsys * sizeof(int), W.stream));
+    CK(cudaStreamSynchronize(W.stream));
+    W.buckets_dirty = true;
+    return 0;
+}
+
+// Restore positions, velocities and FIRE state from the copy kept at upload (device to device).
+int mmff_systems_restore(void) {
+    if (ensure_ready()) return -1;
+    if (!W.nsys) return fail("no systems uploaded");
+    CK(cudaMemcpyAsync(W.d_pos.p, W.d_pos0.p, W.NV * sizeof(float4), cudaMemcpyDeviceToDevice, W.stream));
+    CK(cudaMemcpyAsync(W.d_vel.p, W.d_vel0.p, W.NV * sizeof(float4), cudaMemcpyDeviceToDevice, W.stream));
+    CK(cudaMemcpyAsync(W.d_fire.p, W.d_fire0.p, W.nsys * sizeof(double4), cudaMemcpyDeviceToDevice, W.stream));
+    CK(cudaMemsetAsync(W.d_status.p, 0, W.nsys * sizeof(int), W.stream));
+    return 0;
+}
+
+// Overwrite positions (and velocities, or zero them) of all systems; FIRE state reset.
+int mmff_systems_set_state(const double* pos, const double* vel, int reset_fire) {
+    if (ensure_ready()) return -1;
+    if (!W.nsys) return fail("no systems uploaded");
+    std::vector<float4> hpos(W.NV), hvel(W.NV);
+    for (int s = 0; s < W.nsys; s++) {
+        const int v0 = W.desc[s].z, na = W.natoms[s], nn = W.nnode[s];
+        const double* c = W.orig.data() + 3 * s;
+        for (int i = 0; i < na + nn; i++) {
+            const double* p = pos + 3 * (v0 + i);
+            hpos[v0 + i] = (i < na) ? make_float4((float)(p[0] - c[0]), (float)(p[1] - c[1]), (float)(p[2] - c[2]), 0.f)
+                                    : make_float4((float)p[0], (float)p[1], (float)p[2], 0.f);
+            const double* v = vel ? vel + 3 * (v0 + i) : nullptr;
+            hvel[v0 + i] = v ? make_float4((float)v[0], (float)v[1], (float)v[2], 0.f) : make_float4(0, 0, 0, 0);
+        }
+    }
+    CK(cudaMemcpyAsync(W.d_pos.p, hpos.data(), W.NV * sizeof(float4), cudaMemcpyHostToDevice, W.stream));
+    CK(cudaMemcpyAsync(W.d_vel.p, hvel.data(), W.NV * sizeof(float4), cudaMemcpyHostToDevice, W.stream));
+    if (reset_fire) {
+        std::vector<double4> hf(W.nsys, make_double4(W.fire[0], W.fire[2], 0.0, 0.0));
+        CK(cudaMemcpyAsync(W.d_fire.p, hf.data(), W.nsys * sizeof(double4), cudaMemcpyHostToDevice, W.stream));
+    }
+    CK(cudaStreamSynchronize(W.stream));
+    return 0;
+}
+
+int mmff_eval(int with_energy) {
+    if (ensure_ready()) return -1;
+    if (!W.nsys) return fail("no systems uploaded");
+    if (W.buckets_dirty && build_buckets()) return -1;
+    Params P = make_params(true, 0, 0.0, 0);
+    Systems Y = make_systems();
+    for (auto& B : W.buckets) {
+        void* fn = eval_fn(B.T, B.S, with_energy != 0);
+        const int* q = B.queue.p;
+        int nq = (int)B.sys.size();
+        int mna = B.maxNA, mnn = B.maxNN;
+        void* args[] = {&P, &Y, &q, &nq, &mna, &mnn};
+        CK(cudaLaunchKernel(fn, dim3(nq), dim3(B.T), args, B.smem, W.stream));
+    }
+    CK(cudaGetLastError());
+    return 0;
+}
+
+// Relax every system for up to nstep_max FIRE steps (persistent, one launch per
+// size bucket, buckets run concurrently on their own streams).
+int mmff_relax(int nstep_max, double Fconv, int conv_mode) {
+    if (ensure_ready()) return -1;
+    if (!W.nsys) return fail("no systems uploaded");
+    if (W.buckets_dirty && build_buckets()) return -1;
+    Params P = make_params(false, nstep_max, Fconv, conv_mode);
+    Systems Y = make_systems();
+    CK(cudaMemsetAsync(W.d_counter.p, 0, 64 * sizeof(int), W.stream));
+    CK(cudaEventRecord(W.evfork, W.stream));
+    for (size_t b = 0; b < W.buckets.size(); b++) {
+        Bucket& B = W.buckets[b];
+        cudaStream_t st = W.bstreams[b];
+        CK(cudaStreamWaitEvent(st, W.evfork, 0));
+        void* fn = relax_fn(B.T, B.S, W.count);
+        const int* q = B.queue.p;
+        int nq = (int)B.sys.size();
+        int* ctr = W.d_counter.p + b;
+        int mna = B.maxNA, mnn = B.maxNN;
+        void* args[] = {&P, &Y, &q, &nq, &ctr, &mna, &mnn};
+        CK(cudaLaunchKernel(fn, dim3(B.grid), dim3(B.T), args, B.smem, st));
+    }
+    // join the bucket streams back into the library stream
+    for (size_t b = 0; b < W.buckets.size(); b++) {
+        CK(cudaEventRecord(W.bev[b], W.bstreams[b]));
+        CK(cudaStreamWaitEvent(W.stream, W.bev[b], 0));
+    }
+    CK(cudaGetLastError());
+    return 0;
+}
+
+int mmff_get_forces(double* force) {
+    if (mmff_sync()) return -1;
+    std::vector<float4> h(W.NV);
+    CK(cudaMemcpy(h.data(), W.d_force.p, W.NV * sizeof(float4), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < W.NV; i++) { force[3 * i] = h[i].x; force[3 * i + 1] = h[i].y; force[3 * i + 2] = h[i].z; }
+    return 0;
+}
+
+int mmff_get_energies(double* E) {
+    if (mmff_sync()) return -1;
+    CK(cudaMemcpy(E, W.d_energy.p, W.nsys * sizeof(double4), cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int mmff_get_state(double* pos, double* vel, double* fire, int* status, int* nsteps, double* fconv) {
+    if (mmff_sync()) return -1;
+    if (pos || vel) {
+        std::vector<float4> hp(W.NV), hv(W.NV);
+        CK(cudaMemcpy(hp.data(), W.d_pos.p, W.NV * sizeof(float4), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(hv.data(), W.d_vel.p, W.NV * sizeof(float4), cudaMemcpyDeviceToHost));
+        for (int s = 0; s < W.nsys; s++) {
+            const int v0 = W.desc[s].z, na = W.natoms[s], nn = W.nnode[s];
+            const double* c = W.orig.data() + 3 * s;
+            for (int i = 0; i < na + nn; i++) {
+                const float4 p = hp[v0 + i], v = hv[v0 + i];
+                if (pos) {
+                    if (i < na) { pos[3 * (v0 + i)] = c[0] + p.x; pos[3 * (v0 + i) + 1] = c[1] + p.y; pos[3 * (v0 + i) + 2] = c[2] + p.z; }
+                    else { pos[3 * (v0 + i)] = p.x; pos[3 * (v0 + i) + 1] = p.y; pos[3 * (v0 + i) + 2] = p.z; }
+                }
+                if (vel) { vel[3 * (v0 + i)] = v.x; vel[3 * (v0 + i) + 1] = v.y; vel[3 * (v0 + i) + 2] = v.z; }
+            }
+        }
+    }
+    if (fire) CK(cudaMemcpy(fire, W.d_fire.p, W.nsys * sizeof(double4), cudaMemcpyDeviceToHost));
+    if (status) CK(cudaMemcpy(status, W.d_status.p, W.nsys * sizeof(int), cudaMemcpyDeviceToHost));
+    if (nsteps) CK(cudaMemcpy(nsteps, W.d_nsteps.p, W.nsys * sizeof(int), cudaMemcpyDeviceToHost));
+    if (fconv) {
+        std::vector<float> h(W.nsys);
+        CK(cudaMemcpy(h.data(), W.d_fconv.p, W.nsys * sizeof(float), cudaMemcpyDeviceToHost));
+        for (int s = 0; s < W.nsys; s++) fconv[s] = h[s];
+    }
+    return 0;
+}
+
+// B-spline sample at n points (absolute coordinates) with per-point PLQ: fe[n*4]
+int mmff_grid_sample(int n, const double* pos, const double* PLQ, double* fe) {
+    if (ensure_ready()) return -1;
+    if (!W.grid.p) return fail("no grid");
+    std::vector<float4> hp(n), hq(n), hf(n);
+    for (int i = 0; i < n; i++) {
+        hp[i] = make_float4((float)(pos[3 * i] - W.gpos0[0]), (float)(pos[3 * i + 1] - W.gpos0[1]), (float)(pos[3 * i + 2] - W.gpos0[2]), 0.f);
+        hq[i] = make_float4((float)PLQ[4 * i], (float)PLQ[4 * i + 1], (float)PLQ[4 * i + 2], (float)PLQ[4 * i + 3]);
+    }
+    DBuf<float4> dp, dq, df;
+    if (dp.ensure(n) || dq.ensure(n) || df.ensure(n)) return -1;
+    CK(cudaMemcpy(dp.p, hp.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dq.p, hq.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+    Params P = make_params(true, 0, 0, 0);
+    grid_sample_kernel<<<(unsigned)((4 * n + 127) / 128), 128, 0, W.stream>>>(P, n, dp.p, dq.p, df.p);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(hf.data(), df.p, n * sizeof(float4), cudaMemcpyDeviceToHost, W.stream));
+    CK(cudaStreamSynchronize(W.stream));
+    for (int i = 0; i < n; i++) { fe[4 * i] = hf[i].x; fe[4 * i + 1] = hf[i].y; fe[4 * i + 2] = hf[i].z; fe[4 * i + 3] = hf[i].w; }
+    dp.release(); dq.release(); df.release();
+    return 0;
+}
+
+// CUDA-event timing on the library stream
+int mmff_timer_start(void) {
+    if (ensure_ready()) return -1;
+    CK(cudaEventRecord(W.ev0, W.stream));
+    return 0;
+}
+double mmff_timer_stop(void) {
+    if (cudaEventRecord(W.ev1, W.stream) != cudaSuccess) return -1.0;
+    if (cudaEventSynchronize(W.ev1) != cudaSuccess) return -1.0;
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, W.ev0, W.ev1) != cudaSuccess) return -1.0;
+    return ms;
+}
+
+// Counting mode: the relax kernels also count pair-images inside the cutoff,
+// atom grid samples and force evaluations (for the roofline's algorithmic work).
+int mmff_set_counting(int on) {
+    if (ensure_ready()) return -1;
+    W.count = on != 0;
+    if (W.d_stats.ensure(8)) return -1;
+    CK(cudaMemsetAsync(W.d_stats.p, 0, 8 * sizeof(unsigned long long), W.stream));
+    return 0;
+}
+int mmff_get_counters(unsigned long long* out) {
+    if (mmff_sync()) return -1;
+    CK(cudaMemcpy(out, W.d_stats.p, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int mmff_num_buckets(void) { return W.buckets_dirty ? -1 : (int)W.buckets.size(); }
+int mmff_bucket_info(int b, int* info) {
+    if (b < 0 || b >= (int)W.buckets.size()) return fail("bad bucket");
+    const Bucket& B = W.buckets[b];
+    info[0] = B.T; info[1] = B.S; info[2] = (int)B.sys.size(); info[3] = B.maxNA; info[4] = B.maxNN; info[5] = B.smem; info[6] = B.grid;
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,168 @@
+"""Python host side of the B200 relaxer: a thin wrapper over the C-ABI of
+``libMMFFmulti_lib.so`` (``include/MMFFmulti_lib.h``).
+
+There is no CPU fallback: every compute call goes to the CUDA kernels and
+raises ``RuntimeError`` if the library or a CUDA device is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from .systems import GridSpec, Substrate, SystemBatch
+
+# flag bits (include/MMFFmulti_lib.h, mmff_set_params)
+BONDS, PIPI, PISIGMA, ANGLES = 1, 2, 4, 8
+SUB_ANGLE_NB, SUB_BOND_NB, CLAMP_NB = 16, 32, 64
+NONBONDED, GRID, PBC = 128, 256, 512
+# MolWorld_sp3::run_no_omp with bNonBondNeighs (ForceField.h:170-186)
+DEFAULT_FLAGS = BONDS | PIPI | PISIGMA | ANGLES | SUB_ANGLE_NB | NONBONDED | GRID | PBC
+
+STATUS_CONVERGED, STATUS_MAXSTEPS, STATUS_NAN = 1, 2, -1
+
+
+@dataclass
+class FireParams:
+    """FIRE parameters; defaults = DynamicOpt after setTimeSteps(0.1)
+    (cpp/common/math/DynamicOpt.h:73-95,199-205).  Flim > 0 clamps each
+    assembled force vector as relax_multi.cl:980-983 does."""
+    dt_max: float = 0.1
+    dt_min: float = 0.01
+    damp_max: float = 0.1
+    finc: float = 1.1
+    fdec: float = 0.5
+    falpha: float = 0.8
+    minLastNeg: int = 3
+    cv_kill: float = 0.0
+    Flim: float = -1.0
+
+
+def _check(rc, what):
+    if rc < 0:
+        raise RuntimeError(f"{what} failed: {_lib.load().mmff_last_error().decode()}")
+    return rc
+
+
+class World:
+    """Device-resident batch of MMFF systems on one GPU."""
+
+    def __init__(self, device: int = 0):
+        self.lib = _lib.load()
+        _check(self.lib.mmff_init_device(device), "mmff_init_device")
+        self.batch: SystemBatch | None = None
+        self.grid: GridSpec | None = None
+
+    # ---------------------------------------------------------------- setup
+    def set_params(self, flags=DEFAULT_FLAGS, npbc=(1, 1, 0), Rcut=-1.0, alphaMorse=1.5, FmaxNonBonded=10.0):
+        npbc = np.ascontiguousarray(npbc, np.int32)
+        _check(self.lib.mmff_set_params(flags, _lib.ptr(npbc), Rcut, alphaMorse, FmaxNonBonded), "mmff_set_params")
+
+    def set_fire(self, F: FireParams = FireParams()):
+        _check(self.lib.mmff_set_fire(F.dt_max, F.dt_min, F.damp_max, F.finc, F.fdec, F.falpha, int(F.minLastNeg),
+                                      F.cv_kill, F.Flim), "mmff_set_fire")
+
+    def set_launch(self, threads=0, pair_split=0):
+        _check(self.lib.mmff_set_launch(threads, pair_split), "mmff_set_launch")
+
+    def grid_upload(self, coefs: np.ndarray, grid: GridSpec):
+        c = np.ascontiguousarray(coefs, np.float64)
+        assert c.shape == (grid.n[0], grid.n[1], grid.n[2], 3)
+        p0 = np.array(grid.pos0, np.float64); st = np.array(grid.step, np.float64)
+        _check(self.lib.mmff_grid_upload(int(grid.n[0]), int(grid.n[1]), int(grid.n[2]), _lib.ptr(p0), _lib.ptr(st),
+                                         _lib.ptr(c)), "mmff_grid_upload")
+        self.grid = grid
+
+    def grid_build(self, sub: Substrate, return_coefs: bool = False):
+        g = sub.grid
+        spos = np.ascontiguousarray(sub.spos, np.float64); sREQ = np.ascontiguousarray(sub.sREQ, np.float64)
+        lv = np.ascontiguousarray(sub.lvec.reshape(9), np.float64)
+        nm = np.array(sub.nPBC_mors, np.int32); nc = np.array(sub.nPBC_coul, np.int32)
+        p0 = np.array(g.pos0, np.float64); st = np.array(g.step, np.float64)
+        out = np.zeros((g.n[0], g.n[1], g.n[2], 3)) if return_coefs else None
+        _check(self.lib.mmff_grid_build(spos.shape[0], _lib.ptr(spos), _lib.ptr(sREQ), _lib.ptr(lv), _lib.ptr(nm),
+                                        _lib.ptr(nc), sub.alphaMorse, int(g.n[0]), int(g.n[1]), int(g.n[2]),
+                                        _lib.ptr(p0), _lib.ptr(st), _lib.ptr(out)), "mmff_grid_build")
+        self.grid = g
+        return out
+
+    def upload(self, b: SystemBatch, vel=None):
+        arrs = dict(natoms=np.ascontiguousarray(b.natoms, np.int32), nnode=np.ascontiguousarray(b.nnode, np.int32),
+                    pos=np.ascontiguousarray(b.pos, np.float64),
+                    vel=None if vel is None else np.ascontiguousarray(vel, np.float64),
+                    neighs=np.ascontiguousarray(b.neighs, np.int32), neighCell=np.ascontiguousarray(b.neighCell, np.int32),
+                    bkneighs=np.ascontiguousarray(b.bkneighs, np.int32), REQs=np.ascontiguousarray(b.REQs, np.float64),
+                    apars=np.ascontiguousarray(b.apars, np.float64), bLs=np.ascontiguousarray(b.bLs, np.float64),
+                    bKs=np.ascontiguousarray(b.bKs, np.float64), Ksp=np.ascontiguousarray(b.Ksp, np.float64),
+                    Kpp=np.ascontiguousarray(b.Kpp, np.float64), lvec=np.ascontiguousarray(b.lvec.reshape(-1, 9), np.float64))
+        a = arrs
+        _check(self.lib.mmff_systems_upload(b.nsys, _lib.ptr(a["natoms"]), _lib.ptr(a["nnode"]), _lib.ptr(a["pos"]),
+                                            _lib.ptr(a["vel"]), _lib.ptr(a["neighs"]), _lib.ptr(a["neighCell"]),
+                                            _lib.ptr(a["bkneighs"]), _lib.ptr(a["REQs"]), _lib.ptr(a["apars"]),
+                                            _lib.ptr(a["bLs"]), _lib.ptr(a["bKs"]), _lib.ptr(a["Ksp"]),
+                                            _lib.ptr(a["Kpp"]), _lib.ptr(a["lvec"])), "mmff_systems_upload")
+        self.batch = b
+
+    def restore(self):
+        _check(self.lib.mmff_systems_restore(), "mmff_systems_restore")
+
+    def set_state(self, pos, vel=None, reset_fire=True):
+        pos = np.ascontiguousarray(pos, np.float64)
+        vel = None if vel is None else np.ascontiguousarray(vel, np.float64)
+        _check(self.lib.mmff_systems_set_state(_lib.ptr(pos), _lib.ptr(vel), int(reset_fire)), "mmff_systems_set_state")
+
+    # ---------------------------------------------------------------- compute
+    def eval(self, energy: bool = True):
+        """Forces [sum nvecs, 3] (float64 copies of the FP32 results) and energies [nsys, 4]."""
+        _check(self.lib.mmff_eval(int(energy)), "mmff_eval")
+        b = self.batch
+        F = np.zeros((int(b.nvecs.sum()), 3))
+        _check(self.lib.mmff_get_forces(_lib.ptr(F)), "mmff_get_forces")
+        E = None
+        if energy:
+            E = np.zeros((b.nsys, 4))
+            _check(self.lib.mmff_get_energies(_lib.ptr(E)), "mmff_get_energies")
+        return F, E
+
+    def relax(self, nstep_max: int, Fconv: float = 1e-4, conv_mode: int = 1, sync: bool = True):
+        _check(self.lib.mmff_relax(int(nstep_max), float(Fconv), int(conv_mode)), "mmff_relax")
+        if sync:
+            self.sync()
+
+    def sync(self):
+        _check(self.lib.mmff_sync(), "mmff_sync")
+
+    def state(self):
+        b = self.batch
+        nv = int(b.nvecs.sum())
+        pos = np.zeros((nv, 3)); vel = np.zeros((nv, 3)); fire = np.zeros((b.nsys, 4))
+        st = np.zeros(b.nsys, np.int32); ns = np.zeros(b.nsys, np.int32); fc = np.zeros(b.nsys)
+        _check(self.lib.mmff_get_state(_lib.ptr(pos), _lib.ptr(vel), _lib.ptr(fire), _lib.ptr(st), _lib.ptr(ns),
+                                       _lib.ptr(fc)), "mmff_get_state")
+        return dict(pos=pos, vel=vel, fire=fire, status=st, nsteps=ns, fconv=fc)
+
+    def grid_sample(self, pos, PLQ):
+        pos = np.ascontiguousarray(pos, np.float64); PLQ = np.ascontiguousarray(PLQ, np.float64)
+        fe = np.zeros((pos.shape[0], 4))
+        _check(self.lib.mmff_grid_sample(pos.shape[0], _lib.ptr(pos), _lib.ptr(PLQ), _lib.ptr(fe)), "mmff_grid_sample")
+        return fe
+
+    # ---------------------------------------------------------------- timing
+    def timer_start(self):
+        _check(self.lib.mmff_timer_start(), "mmff_timer_start")
+
+    def timer_stop(self) -> float:
+        ms = self.lib.mmff_timer_stop()
+        if ms < 0:
+            raise RuntimeError("mmff_timer_stop failed")
+        return ms
+
+    def buckets(self):
+        out = []
+        for b in range(max(0, self.lib.mmff_num_buckets())):
+            info = np.zeros(7, np.int32)
+            _check(self.lib.mmff_bucket_info(b, _lib.ptr(info)), "mmff_bucket_info")
+            out.append(dict(zip(["threads", "pair_split", "nsys", "maxNA", "maxNN", "smem", "ctas"], info.tolist())))
+        return out

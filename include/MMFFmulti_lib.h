@@ -1,0 +1,143 @@
+/*
+ * MMFFmulti_lib.h -- C-ABI of the B200 multi-system MMFF relaxer
+ * (libMMFFmulti_lib.so, built in-tree by firecore_b200/build.py).
+ *
+ * Two layers:
+ *  1. The CSR world API (mmff_*): uneven systems packed back to back, the
+ *     additive extension the reference's fixed-replica ABI lacks.  Plain
+ *     pointers and sizes; host arrays are FP64 / int32 in the reference's
+ *     MMFFsp3_loc layout (cpp/common/molecular/MMFFsp3_loc.h:43-139).
+ *  2. The legacy symbols pyBall/MMFF_multi.py binds (init, run, eval, ...;
+ *     pyBall/MMFF_multi.py:99-599, cpp/libs_OCL/MMFFmulti_lib.cpp), declared at
+ *     the end, implemented on top of layer 1.
+ *
+ * Error behaviour: every int-returning call returns 0 (or a count) on success
+ * and a negative value on failure, with a message in mmff_last_error(); the
+ * library never exits the process (the reference prints and exit(0)s,
+ * OCL.h OCL_checkError).  Nothing here falls back to the CPU: without a CUDA
+ * device every compute call fails.
+ */
+#ifndef MMFFMULTI_LIB_H
+#define MMFFMULTI_LIB_H
+#include <stdint.h>
+#include <stdbool.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ errors/setup */
+const char* mmff_last_error(void);
+/* Select the CUDA device and create the library stream.
+ * Replaces OCLsystem::init (cpp/common/OpenCL/OCL.h:386-410). */
+int mmff_init_device(int device);
+/* Wait for all queued work; reports asynchronous kernel errors. */
+int mmff_sync(void);
+
+/* ------------------------------------------------------------ switches */
+/* flags: bit set of BONDS 1, PIPI 2, PISIGMA 4, ANGLES 8, SUB_ANGLE_NB 16,
+ * SUB_BOND_NB 32, CLAMP_NB 64, NONBONDED 128, GRID 256, PBC 512 -- the
+ * MMFFsp3_loc do* switches and ForceField::setNonBondStrategy flags
+ * (cpp/common/molecular/ForceField.h:147-186).  nPBC: image counts
+ * (MolWorld_sp3::makePBCshifts, MolWorld_sp3.h:775).  Rcut <= 0: all pairs x
+ * all images (NBFF::evalLJQs_ng4_PBC_atom_omp, NBFF.h:575); Rcut > 0: pairs
+ * beyond Rcut dropped and Coulomb in shifted-force form.  Set before
+ * mmff_systems_upload (neighCell indices are validated against nPBC). */
+int mmff_set_params(int flags, const int* nPBC, double Rcut, double alphaMorse, double FmaxNonBonded);
+/* FIRE parameters (DynamicOpt members, cpp/common/math/DynamicOpt.h:73-95;
+ * set_opt, cpp/libs_OCL/MMFFmulti_lib.cpp:141).  Flim > 0 clamps each
+ * assembled force vector to |f| <= Flim (relax_multi.cl:980-983). */
+int mmff_set_fire(double dt_max, double dt_min, double damp_max, double finc, double fdec, double falpha,
+                  int minLastNeg, double cv_kill, double Flim);
+/* Threads per CTA (64/128/256/512) and lanes per atom in the pair sum
+ * (1/2/4/8); 0 = chosen per size bucket. */
+int mmff_set_launch(int threads, int pair_split);
+
+/* ------------------------------------------------------------ substrate grid */
+/* Upload FP64 B-spline coefficients [nx][ny][nz][3] (z fastest; Pauli,
+ * London, Coulomb), stored on the device as float4.  Replaces the
+ * BsplinePLQ buffer upload of MolWorld_sp3_multi::initGridFF
+ * (cpp/common/molecular/MolWorld_sp3_multi.h:2576-2581). */
+int mmff_grid_upload(int nx, int ny, int nz, const double* pos0, const double* step, const double* coefs);
+/* Build the grid on the GPU in FP64: node potentials of the substrate
+ * (GridFF::evalBsplineRef with bUseEwald=false, GridFF.h:847-891) and the
+ * exact B-spline fit (the limit of Bspline::fit3D_omp, Bspline_fit_3D.h:411).
+ * spos [nsub*3], sREQ [nsub*4], lvec [9]; coefs_out (nullable) receives the
+ * FP64 coefficients [nx][ny][nz][3]. */
+int mmff_grid_build(int nsub, const double* spos, const double* sREQ, const double* lvec, const int* nPBC_mors,
+                    const int* nPBC_coul, double alphaMorse, int nx, int ny, int nz, const double* pos0,
+                    const double* step, double* coefs_out);
+/* B-spline sample (GridFF::getForce_Bspline, GridFF.h:355) at n points:
+ * pos [n*3], PLQ [n*4] -> fe [n*4] = (Fx, Fy, Fz, E). */
+int mmff_grid_sample(int n, const double* pos, const double* PLQ, double* fe);
+
+/* ------------------------------------------------------------ systems (CSR) */
+/* Upload nsys systems (replaces MolWorld_sp3_multi::pack_system + upload,
+ * MolWorld_sp3_multi.h:514-703, for uneven sizes).  Per system natoms[s] atoms
+ * (nnode[s] nodes first) and nvecs = natoms + nnode vectors.
+ * pos/vel [sum nvecs][3] (vel nullable = 0); neighs/neighCell/bkneighs
+ * [sum natoms][4] local indices; REQs [sum natoms][4]; apars/bLs/bKs/Ksp/Kpp
+ * [sum nnode][4]; lvec [nsys][9].  Indices are validated. */
+int mmff_systems_upload(int nsys, const int* natoms, const int* nnode, const double* pos, const double* vel,
+                        const int* neighs, const int* neighCell, const int* bkneighs, const double* REQs,
+                        const double* apars, const double* bLs, const double* bKs, const double* Ksp,
+                        const double* Kpp, const double* lvec);
+/* Restore positions, velocities and FIRE state saved at upload (device copy). */
+int mmff_systems_restore(void);
+/* Overwrite positions (and velocities; NULL = 0); reset_fire != 0 resets dt,
+ * damping and lastNeg. */
+int mmff_systems_set_state(const double* pos, const double* vel, int reset_fire);
+
+/* ------------------------------------------------------------ compute */
+/* One force evaluation per system (forces assembled, unclamped) and, with
+ * with_energy, FP64 energies (bonded, non-bonded, grid, total).  The force
+ * phase of MolWorld_sp3::run_no_omp (MolWorld_sp3.h:2305-2386). */
+int mmff_eval(int with_energy);
+/* FIRE relaxation of every system for at most nstep_max steps, stopping a
+ * system when sum f^2 < Fconv^2 (conv_mode 0, MolWorld_sp3.h:2460) or
+ * max |f| < Fconv (conv_mode 1).  Replaces run_ocl_opt
+ * (MolWorld_sp3_multi.h:1694-1846) with per-system FIRE in FP64 on the device
+ * and no host round trip.  Asynchronous: mmff_sync / mmff_get_* wait. */
+int mmff_relax(int nstep_max, double Fconv, int conv_mode);
+
+/* ------------------------------------------------------------ results */
+int mmff_get_forces(double* force);                 /* [sum nvecs][3] */
+int mmff_get_energies(double* E);                   /* [nsys][4] */
+/* pos/vel [sum nvecs][3] absolute frame; fire [nsys][4] (dt, damping, lastNeg,
+ * total steps); status [nsys] (1 converged, 2 step limit, -1 NaN);
+ * nsteps [nsys] (run_no_omp's return value); fconv [nsys] (convergence
+ * measure at exit).  Any pointer may be NULL. */
+int mmff_get_state(double* pos, double* vel, double* fire, int* status, int* nsteps, double* fconv);
+
+/* ------------------------------------------------------------ timing / info */
+int mmff_timer_start(void);                          /* CUDA event on the library stream */
+double mmff_timer_stop(void);                        /* ms since mmff_timer_start, <0 on error */
+/* Counting mode (on != 0): the relax kernels also count pair-images inside
+ * the cutoff, atom B-spline samples and force evaluations; counters reset. */
+int mmff_set_counting(int on);
+/* out[3] = (pair-images, atom grid samples, force evaluations) since the reset */
+int mmff_get_counters(unsigned long long* out);
+/* Measured denominators: FP32 FFMA throughput [TFLOP/s] and L2-resident
+ * float4 read bandwidth [GB/s] over an mbytes MiB buffer; < 0 on error. */
+double mmff_peak_fp32(void);
+double mmff_peak_l2(int mbytes);
+int mmff_num_buckets(void);
+/* info[7] = (threads, pair_split, nsys, maxNA, maxNN, smem bytes, CTAs) */
+int mmff_bucket_info(int b, int* info);
+
+/* ------------------------------------------------------------ synthetic workloads */
+/* Node count the generator produces for natoms atoms. */
+int mmff_gen_nnode(int natoms);
+/* Seeded molecules (C:N:O:H = 10:2:2:10 heavy-atom trees with H caps) in the
+ * layout above; topo_mode 0 = replicas of one topology, 1 = one per system. */
+int mmff_gen_systems(int nsys, const int* natoms, uint64_t seed, int topo_mode, double sigma, int rotate,
+                     double zplace, const double* cell_xy, int hbond, double* pos, int* neighs, int* neighCell,
+                     int* bkneighs, double* REQs, double* apars, double* bLs, double* bKs, double* Ksp, double* Kpp,
+                     int* elements, int central_cell);
+/* Rock-salt (001) slab; returns the number of ions. */
+int mmff_gen_slab(double a, int ncell, int layers, double z_top, double q, const double* REQ_cation,
+                  const double* REQ_anion, double* spos, double* sREQ);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -7,9 +7,10 @@
  * so that FP64 results agree to rounding with the compiled reference harness
  * (oracle/ref_harness.cpp) on the golden fixtures.
  *
- * Extension beyond the reference (documented, off by default): an optional
- * smooth non-bonded cutoff (P->Rcut > 0).  With Rcut <= 0 the pair sum is the
- * reference's all-pairs x all-images sum.
+ * Extensions beyond the reference (both off by default): a non-bonded cutoff
+ * (P->Rcut > 0, Coulomb in shifted-force form) and a per-vector force clamp in
+ * FIRE (F->Flim > 0, as relax_multi.cl:980-983).  With Rcut <= 0 the pair sum
+ * is the reference's all-pairs x all-images sum.
  */
 #include "mmff_oracle.h"
 #include <math.h>
@@ -235,15 +236,6 @@ static double eval_atom(const sysview* S, const ORC_params* P, int ia) {
     return E;
 }
 
-/* Smooth cutoff switch on r^2 (extension; not in the reference). */
-static inline double switch_r2(double r2, double Ron2, double inv_w, double* dSdr2) {
-    double t = (r2 - Ron2) * inv_w;
-    if (t <= 0) { *dSdr2 = 0; return 1.0; }
-    if (t >= 1) { *dSdr2 = 0; return 0.0; }
-    *dSdr2 = -6.0 * t * (1.0 - t) * inv_w;
-    return 1.0 - t * t * (3.0 - 2.0 * t);
-}
-
 /* NBFF.h:575-618 evalLJQs_ng4_PBC_atom_omp (returns 0.5*E; adds force) */
 static double eval_nb_atom(const sysview* S, const ORC_params* P, int ia) {
     const v3 pi = ld3(S->pos + 3 * ia);
@@ -254,8 +246,6 @@ static double eval_nb_atom(const sysview* S, const ORC_params* P, int ia) {
     const int npbc = usePBC ? S->npbc : 1;
     const int cut = P->Rcut > 0;
     const double Rc2 = P->Rcut * P->Rcut;
-    const double Ron2 = P->Ron * P->Ron;
-    const double inv_w = cut ? 1.0 / (Rc2 - Ron2) : 0.0;
     double E = 0, fx = 0, fy = 0, fz = 0;
     for (int j = 0; j < S->natoms; j++) {
         if (ia == j) continue;
@@ -275,12 +265,16 @@ static double eval_nb_atom(const sysview* S, const ORC_params* P, int ia) {
             v3 fij;
             double eij;
             if (cut) {
+                /* extension: pairs beyond Rcut dropped; Coulomb in shifted-force
+                 * form so the force is continuous at Rcut:
+                 * E = kQ (1/r - 1/Rc + (r - Rc)/Rc^2), F = kQ (1/r^2 - 1/Rc^2) */
                 double r2 = vdot(dpc, dpc);
                 if (r2 >= Rc2) continue;
                 eij = getLJQH(dpc, REQij, &fij);
-                double dS; double Sw = switch_r2(r2, Ron2, inv_w, &dS);
-                fij = vaddmul(vmul(fij, Sw), dpc, 2.0 * eij * dS);
-                eij *= Sw;
+                const double r = sqrt(r2);
+                const double kQ = COULOMB_CONST * REQij[2];
+                fij = vaddmul(fij, dpc, kQ / (Rc2 * r));
+                eij += kQ * (r - 2.0 * P->Rcut) / Rc2;
             } else {
                 eij = getLJQH(dpc, REQij, &fij);
             }

@@ -48,8 +48,9 @@ enum {
 typedef struct {
     int    flags;
     int    npbc[3];        /* nPBC image counts, images run -n..n        */
-    double Rcut;           /* <=0: no cutoff (reference semantics)      */
-    double Ron;            /* switching starts here (Ron<Rcut)          */
+    double Rcut;           /* <=0: no cutoff (reference semantics); >0: pairs
+                              beyond Rcut dropped, shifted-force Coulomb */
+    double Ron;            /* unused (kept for layout)                  */
     double FmaxNonBonded;  /* clamp for bClampNonBonded                 */
     double alphaMorse;     /* REQ -> PLQ conversion exponent            */
     /* grid */

@@ -1,0 +1,181 @@
+"""CUDA path (through the C-ABI) against the FP64 oracle and the reference's
+golden outputs.  Tolerances (FP32 forces, FP64 reductions):
+  forces   : max_i |F_gpu - F_ref| <= FTOL * max_i |F_ref|   per system
+  energies : |E_gpu - E_ref| <= ETOL * (|E_bonded| + |E_nb| + |E_grid|)
+  relaxed  : final energy within 1e-5 eV/atom, RMSD <= 1e-3 A
+"""
+import numpy as np
+import pytest
+
+from conftest import batch_from_golden, grid_from_golden
+from firecore_b200 import systems as S
+from firecore_b200.world import DEFAULT_FLAGS, GRID, PBC, FireParams, World
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+FTOL = 1e-5
+ETOL = 1e-5
+FLAGSETS = {"full": DEFAULT_FLAGS, "nogrid": DEFAULT_FLAGS & ~GRID, "nopbc": DEFAULT_FLAGS & ~PBC & ~GRID}
+
+
+@pytest.fixture(scope="module")
+def world(golden):
+    w = World(0)
+    w.grid_upload(golden["C"], grid_from_golden(golden))
+    return w
+
+
+def per_system_force_err(b, F, Fr):
+    a, n, v = b.offsets()
+    errs = []
+    for s in range(b.nsys):
+        d = np.abs(F[v[s]:v[s + 1]] - Fr[v[s]:v[s + 1]]).max()
+        errs.append(d / max(np.abs(Fr[v[s]:v[s + 1]]).max(), 1e-12))
+    return np.array(errs)
+
+
+def check_eval(world, b, grid, C, flags, npbc=(1, 1, 0), Rcut=-1.0):
+    world.set_params(flags=flags, npbc=npbc, Rcut=Rcut)
+    world.upload(b)
+    F, E = world.eval(True)
+    pos = world.state()["pos"]             # the positions the GPU holds (FP32 local frame)
+    P = O.make_params(grid, flags=flags, npbc=npbc, Rcut=Rcut)
+    Fo, Eo = O.eval_forces(b, P, C, pos=pos)
+    ferr = per_system_force_err(b, F, Fo)
+    scale = np.abs(Eo[:, :3]).sum(1)
+    eerr = np.abs(E - Eo).max(1) / np.maximum(scale, 1e-9)
+    return ferr, eerr
+
+
+@pytest.mark.parametrize("tag", ["A", "B"])
+@pytest.mark.parametrize("fset", list(FLAGSETS))
+def test_eval_vs_oracle(world, golden, tag, fset):
+    b = batch_from_golden(golden, tag)
+    ferr, eerr = check_eval(world, b, grid_from_golden(golden), golden["C"], FLAGSETS[fset])
+    assert ferr.max() < FTOL, ferr
+    assert eerr.max() < ETOL, eerr
+
+
+@pytest.mark.parametrize("tag", ["A", "B"])
+def test_eval_vs_reference_golden(world, golden, tag):
+    """Direct comparison with FireCore's own forces at the golden positions
+    (includes the FP32 rounding of the inputs)."""
+    b = batch_from_golden(golden, tag)
+    world.set_params(flags=DEFAULT_FLAGS)
+    world.upload(b)
+    F, E = world.eval(True)
+    ferr = per_system_force_err(b, F, golden[f"{tag}_full_F"])
+    assert ferr.max() < 2e-4, ferr     # input rounding (p ~ 10 A in FP32) x bond stiffness dominates
+    Er = golden[f"{tag}_full_E"]
+    assert np.abs(E[:, 3] - Er[:, 3]).max() / np.abs(Er[:, :3]).sum(1).max() < 1e-5
+
+
+def test_eval_cutoff_vs_oracle(world, golden):
+    b = batch_from_golden(golden, "B")
+    ferr, eerr = check_eval(world, b, grid_from_golden(golden), golden["C"], DEFAULT_FLAGS, Rcut=6.0)
+    assert ferr.max() < FTOL and eerr.max() < ETOL
+
+
+def test_grid_sample_vs_reference(world, golden):
+    fe = world.grid_sample(golden["samp_pos"], golden["samp_PLQ"])
+    ref = golden["samp_fe"]
+    assert np.abs(fe - ref).max() <= 2e-5 * np.abs(ref).max()
+
+
+def test_grid_build_vs_oracle(world, golden):
+    from firecore_b200.systems import Substrate
+    sub = Substrate(golden["spos"], golden["sREQ"], golden["slvec"], grid_from_golden(golden), 1.5, (1, 1, 0), (4, 4, 0))
+    w2 = World(0)
+    C = w2.grid_build(sub, return_coefs=True)
+    ref = golden["C"]
+    assert np.abs(C - ref).max() <= 1e-9 * np.abs(ref).max()
+    # restore the module grid for later tests
+    world.grid_upload(golden["C"], grid_from_golden(golden))
+
+
+def test_uneven_batch_vs_oracle(world, golden):
+    sizes = [20, 33, 57, 64, 65, 120, 128, 129, 200, 256, 257, 400]
+    b = S.make_systems(sizes, seed=3, topo_mode=1, sigma=0.1, cell=(11.28, 11.28, 40.0), npbc=(0, 0, 0))
+    ferr, eerr = check_eval(world, b, grid_from_golden(golden), golden["C"], DEFAULT_FLAGS, npbc=(0, 0, 0), Rcut=8.0)
+    assert ferr.max() < FTOL, ferr
+    assert eerr.max() < ETOL, eerr
+
+
+def test_relax_vs_oracle(world, golden):
+    """Full relaxation (max |f| < 1e-4, Flim = 10): final energy and geometry."""
+    grid = grid_from_golden(golden)
+    b = batch_from_golden(golden, "A")
+    world.set_params(flags=DEFAULT_FLAGS)
+    fp = FireParams(Flim=10.0)
+    world.set_fire(fp)
+    world.upload(b)
+    pos0 = world.state()["pos"]
+    world.relax(6000, 1e-4, conv_mode=1)
+    st = world.state()
+    P = O.make_params(grid)
+    Fo = O.make_fire(Flim=10.0)
+    r = O.relax(b, P, Fo, golden["C"], niter=6000, Fconv=1e-4, conv_mode=1, pos=pos0)
+    assert (st["status"] == 1).all(), st["status"]
+    assert (r["converged"] == 1).all()
+    a, n, v = b.offsets()
+    _, Eg = O.eval_forces(b, P, golden["C"], pos=st["pos"])
+    _, Ec = O.eval_forces(b, P, golden["C"], pos=r["pos"])
+    for s in range(b.nsys):
+        na = b.natoms[s]
+        dE = abs(Eg[s, 3] - Ec[s, 3]) / na
+        d = st["pos"][v[s]:v[s] + na] - r["pos"][v[s]:v[s] + na]
+        rmsd = np.sqrt((d ** 2).sum(1).mean())
+        assert dE <= 1e-5, (s, dE)
+        assert rmsd <= 1e-3, (s, rmsd)
+    world.set_fire(FireParams())
+
+
+def test_relax_steps_match_reference_semantics(world, golden):
+    """nsteps / status bookkeeping of run_no_omp: converged systems report the
+    index of the converging step; unconverged ones the step limit."""
+    b = batch_from_golden(golden, "A")
+    world.set_params(flags=DEFAULT_FLAGS)
+    world.set_fire(FireParams(Flim=10.0))
+    world.upload(b)
+    world.relax(50, 1e-4, conv_mode=0)
+    st = world.state()
+    assert (st["status"] == 2).all() and (st["nsteps"] == 50).all()
+    assert np.allclose(st["fire"][:, 3], 50)
+    world.relax(50, 1e-4, conv_mode=0)          # continues from the saved state
+    assert np.allclose(world.state()["fire"][:, 3], 100)
+    world.set_fire(FireParams())
+
+
+def test_nan_system_is_retired_not_fatal(world, golden):
+    """Failure detection: a system with two atoms on the same spot produces
+    non-finite forces; it is flagged (status -1) and the others relax."""
+    b = S.make_systems([24, 24, 24], seed=5, topo_mode=0, sigma=0.05, cell=(11.28, 11.28, 40.0))
+    a, n, v = b.offsets()
+    b.pos[v[1] + 20] = b.pos[v[1] + 21]          # two caps of system 1 coincide
+    world.set_params(flags=DEFAULT_FLAGS)
+    world.set_fire(FireParams(Flim=10.0))
+    world.upload(b)
+    world.relax(300, 1e-4, conv_mode=1)
+    st = world.state()
+    assert st["status"][1] == -1
+    assert st["status"][0] in (1, 2) and st["status"][2] in (1, 2)
+    world.set_fire(FireParams())
+
+
+def test_queue_claims_every_system_once(world, golden):
+    """More systems than resident CTAs: the persistent queue processes each once."""
+    b = S.make_systems([24] * 3000, seed=9, topo_mode=0, sigma=0.05, cell=(11.28, 11.28, 40.0))
+    world.set_params(flags=DEFAULT_FLAGS)
+    world.upload(b)
+    world.relax(7, 1e-12, conv_mode=1)
+    st = world.state()
+    assert (st["status"] == 2).all() and (st["nsteps"] == 7).all()
+    assert np.allclose(st["fire"][:, 3], 7)
+
+
+def test_bad_topology_rejected(world):
+    b = S.make_systems([24], seed=1, cell=(11.28, 11.28, 40.0))
+    b.neighs[3, 0] = 99                             # out of range
+    with pytest.raises(RuntimeError, match="out of range"):
+        world.upload(b)
