@@ -347,6 +347,7 @@ def run_reference(args):
 
 
 def main():
+    global MAXSTEPS
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -355,7 +356,9 @@ def main():
     ap.add_argument("--nsys", type=int, default=4096)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--maxsteps", type=int, default=MAXSTEPS, help="FIRE step limit per system (profiling runs use fewer)")
     args = ap.parse_args()
+    MAXSTEPS = args.maxsteps
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -3,6 +3,9 @@
 #pragma once
 #include <cstdint>
 
+// Set the message mmff_last_error() returns (C++ linkage, internal to the library).
+void mmff_set_error(const char* msg);
+
 extern "C" {
 
 // Node (heavy atom) count the generator produces for a molecule of natoms atoms.

@@ -17,6 +17,7 @@
 
 #include "MMFFmulti_lib.h"
 #include "mmff_device.cuh"
+#include "mmff_host.h"
 
 namespace mmff {
 // kernels (mmff_relax.cu, mmff_grid.cu)
@@ -212,6 +213,8 @@ template <class X> int upload(DBuf<X>& d, const std::vector<X>& h) {
 }
 
 }  // namespace
+
+void mmff_set_error(const char* msg) { g_err = msg; }
 
 // ============================================================================ C-ABI
 extern "C" {
