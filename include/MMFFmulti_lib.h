@@ -66,6 +66,20 @@ int mmff_grid_upload(int nx, int ny, int nz, const double* pos0, const double* s
 int mmff_grid_build(int nsub, const double* spos, const double* sREQ, const double* lvec, const int* nPBC_mors,
                     const int* nPBC_coul, double alphaMorse, int nx, int ny, int nz, const double* pos0,
                     const double* step, double* coefs_out);
+/* No counterpart in the reference.  In-place B-spline fit of a device array
+ * the caller owns, for callers that may not allocate device memory (their
+ * memory comes from a fixed arena they manage, so a cudaMalloc inside the
+ * library would break their budget): d_coefs [nx][ny][nz][3] FP64 holds the
+ * node values on entry and the coefficients on exit; nothing is allocated.
+ * Limit: at most 4096 points per axis (larger grids return an error).  The
+ * solver coefficients live in one static device array per GPU that the
+ * library keeps until exit; every call rewrites them before use, and calls
+ * whose kernels overlap on the GPU (different streams) race on it.  The
+ * first call on a device looks up that array's device address
+ * (cudaGetSymbolAddress) with the device current; make that first call
+ * before any stream capture.  Kernels run on `stream` (a cudaStream_t;
+ * NULL = legacy default stream); the call does not synchronise. */
+int mmff_bspline_fit_noalloc(double* d_coefs, int nx, int ny, int nz, void* stream);
 /* B-spline sample (GridFF::getForce_Bspline, GridFF.h:355) at n points:
  * pos [n*3], PLQ [n*4] -> fe [n*4] = (Fx, Fy, Fz, E). */
 int mmff_grid_sample(int n, const double* pos, const double* PLQ, double* fe);
