@@ -7,7 +7,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libMMFFmulti_lib.so")
+LIB_PATH = os.environ.get("MMFF_LIB", os.path.join(HERE, "libMMFFmulti_lib.so"))
 _lib = None
 
 
@@ -46,7 +46,7 @@ def _declare(lib):
     lib.mmff_last_error.restype = ctypes.c_char_p
     sig = {
         "mmff_init_device": [c_int], "mmff_sync": [], "mmff_set_params": [c_int, c_void, c_double, c_double, c_double],
-        "mmff_set_fire": [c_double] * 6 + [c_int, c_double, c_double], "mmff_set_launch": [c_int, c_int],
+        "mmff_set_fire": [c_double] * 6 + [c_int, c_double, c_double, c_int], "mmff_set_launch": [c_int, c_int],
         "mmff_grid_upload": [c_int, c_int, c_int, c_void, c_void, c_void],
         "mmff_grid_build": [c_int, c_void, c_void, c_void, c_void, c_void, c_double, c_int, c_int, c_int, c_void,
                             c_void, c_void],

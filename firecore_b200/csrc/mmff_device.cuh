@@ -45,6 +45,7 @@ struct Params {
     // FIRE
     double dt_max, dt_min, damp_max, finc, fdec, falpha, cv_kill;
     int minLastNeg;
+    int fire_variant;    // 0: run_no_omp mixing f*(dt + renorm*cf); 1: Bitzek 2006 mixing f*(dt + cf)
     float Flim;          // <=0: no force clamp
     double Fconv2;
     int conv_mode;       // 0: sum f^2 ; 1: max |f|^2
@@ -325,6 +326,26 @@ __host__ __device__ inline SmemLayout smem_layout(int maxNA, int maxNN, int T) {
     L.fng = take(16 * 8 * maxNN);
     L.red = take(128 * L.nwarps + 64);     // per warp: 4 doubles (32 B) at 0, bbox 6 floats at 64*nwarps
     L.total = o;
+    return L;
+}
+
+// ---- shared-memory carve-up of one warp-per-system region (byte offsets)
+struct WarpLayout {
+    int pos, REQ, fng, misc, ng, ngC, bk, npar, per_warp;   // byte offsets inside one warp's region
+};
+__host__ __device__ inline WarpLayout warp_layout(int maxNA, int maxNN) {
+    WarpLayout L;
+    int o = 0;
+    auto take = [&](int b) { int r = o; o += (b + 15) & ~15; return r; };
+    L.pos = take(16 * (maxNA + maxNN));
+    L.REQ = take(16 * maxNA);
+    L.fng = take(16 * 8 * maxNN);
+    L.misc = take(16 * 4);          // lattice vectors (9 floats) + grid offset (3 floats)
+    L.ng = take(16 * maxNA);
+    L.ngC = take(16 * maxNA);
+    L.bk = take(16 * maxNA);
+    L.npar = take(16 * 5 * maxNN);  // apars, bLs, bKs, Ksp, Kpp per node
+    L.per_warp = o;
     return L;
 }
 

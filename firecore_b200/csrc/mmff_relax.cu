@@ -433,7 +433,7 @@ __global__ void __launch_bounds__(T) relax_kernel(Params P, Systems Y, const int
                 lastNeg++;
             }
             float mn[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, mx[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
-            E.move(dt, cv, renorm_vf * cf, mn, mx);
+            E.move(dt, cv, P.fire_variant == 1 ? cf : renorm_vf * cf, mn, mx);
             total += 1.0;
             const double m = (P.conv_mode == 0) ? ff : (double)fmax2;
             meas = (float)sqrt(m);

@@ -31,6 +31,9 @@ __global__ void solve_periodic_kernel(double*, long, int, long, long, int, long,
 __global__ void pack_grid_kernel(long, const double*, float4*);
 void* relax_fn(int T, int S, bool count);
 void* eval_fn(int T, int S, bool energy);
+void* relax_warp_fn(int apl, bool count);
+void* eval_warp_fn(int apl, bool energy);
+
 }  // namespace mmff
 
 using namespace mmff;
@@ -62,6 +65,8 @@ template <class X> struct DBuf {
 };
 
 struct Bucket {
+    int kind = 0;                  // 0: CTA per system (T threads, S lanes per atom); 1: warp per system
+    int apl = 1;                   // warp engine: atoms per lane (1: <=32 atoms, 2: <=64)
     int T = 64, S = 1, maxNA = 0, maxNN = 0;
     std::vector<int> sys;          // system indices, largest first
     DBuf<int> queue;
@@ -97,7 +102,7 @@ struct World {
     int flags = F_BONDS | F_PIPI | F_PISIGMA | F_ANGLES | F_SUB_ANGLE_NB | F_NONBONDED | F_GRID | F_PBC;
     int npbc[3] = {1, 1, 0};
     double Rcut = -1.0, alphaMorse = 1.5, FmaxNB = 10.0;
-    double fire[9] = {0.1, 0.01, 0.1, 1.1, 0.5, 0.8, 3, 0.0, -1.0};  // dt_max dt_min damp_max finc fdec falpha minLastNeg cv_kill Flim
+    double fire[10] = {0.1, 0.01, 0.1, 1.1, 0.5, 0.8, 3, 0.0, -1.0, 0};  // dt_max dt_min damp_max finc fdec falpha minLastNeg cv_kill Flim variant
     // launch configuration (0 = heuristic)
     int force_T = 0, force_S = 0;
     std::vector<Bucket> buckets;
@@ -138,6 +143,7 @@ Params make_params(bool for_eval, int nstep_max, double Fconv, int conv_mode) {
     P.dt_max = W.fire[0]; P.dt_min = W.fire[1]; P.damp_max = W.fire[2]; P.finc = W.fire[3];
     P.fdec = W.fire[4]; P.falpha = W.fire[5]; P.minLastNeg = (int)W.fire[6]; P.cv_kill = W.fire[7];
     P.Flim = for_eval ? -1.f : (float)W.fire[8];
+    P.fire_variant = (int)W.fire[9];
     P.Fconv2 = Fconv * Fconv;
     P.conv_mode = conv_mode;
     P.nstep_max = nstep_max;
@@ -162,38 +168,58 @@ int pow2_floor(int x) { int p = 1; while (p * 2 <= x) p *= 2; return p; }
 int build_buckets() {
     W.buckets.clear();
     const int Ts[4] = {64, 128, 256, 512};
-    std::vector<std::vector<int>> groups(4);
+    // groups 0/1: warp engine (<=32 / <=64 atoms), 2..5: CTA engine by thread count
+    std::vector<std::vector<int>> groups(6);
     for (int s = 0; s < W.nsys; s++) {
-        int na = W.natoms[s], b = 3;
-        for (int k = 0; k < 4; k++) if (na <= Ts[k]) { b = k; break; }
-        if (W.force_T) { for (int k = 0; k < 4; k++) if (Ts[k] == W.force_T) b = k; }
+        const int na = W.natoms[s];
+        int b;
+        if (!W.force_T && na <= 32) b = 0;
+        else if (!W.force_T && na <= 64) b = 1;
+        else {
+            b = 5;
+            for (int k = 0; k < 4; k++) if (na <= Ts[k]) { b = 2 + k; break; }
+            if (W.force_T) { for (int k = 0; k < 4; k++) if (Ts[k] == W.force_T) b = 2 + k; }
+        }
         groups[b].push_back(s);
     }
     int dev_smem = 0;
     CK(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, W.device));
     int nsm = 0;
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, W.device));
-    for (int k = 3; k >= 0; k--) {
+    // largest systems first: their buckets are launched first
+    for (int k = 5; k >= 0; k--) {
         if (groups[k].empty()) continue;
         Bucket B;
-        B.T = Ts[k];
         B.sys = groups[k];
         std::stable_sort(B.sys.begin(), B.sys.end(), [](int a, int b) { return W.natoms[a] > W.natoms[b]; });
         for (int s : B.sys) { B.maxNA = std::max(B.maxNA, W.natoms[s]); B.maxNN = std::max(B.maxNN, W.nnode[s]); }
-        int S = pow2_floor(std::max(1, B.T / std::max(1, B.maxNA)));
-        B.S = std::min(S, 8);
-        if (W.force_S) B.S = W.force_S;
-        B.smem = smem_layout(B.maxNA, B.maxNN, B.T).total;
+        void* fns[3];
+        if (k <= 1) {
+            B.kind = 1; B.apl = k + 1; B.T = 128; B.S = 1;
+            B.smem = 4 * warp_layout(B.maxNA, B.maxNN).per_warp;
+            fns[0] = relax_warp_fn(B.apl, false); fns[1] = relax_warp_fn(B.apl, true);
+            fns[2] = nullptr;
+        } else {
+            B.kind = 0; B.T = Ts[k - 2];
+            int S = pow2_floor(std::max(1, B.T / std::max(1, B.maxNA)));
+            B.S = std::min(S, 8);
+            if (W.force_S) B.S = W.force_S;
+            B.smem = smem_layout(B.maxNA, B.maxNN, B.T).total;
+            fns[0] = relax_fn(B.T, B.S, false); fns[1] = relax_fn(B.T, B.S, true); fns[2] = nullptr;
+        }
         if (B.smem > dev_smem) return fail("system too large for shared memory: %d B > %d B", B.smem, dev_smem);
-        void* fn = relax_fn(B.T, B.S, false);
-        if (!fn) return fail("no kernel for T=%d S=%d", B.T, B.S);
-        CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, B.smem));
-        CK(cudaFuncSetAttribute(relax_fn(B.T, B.S, true), cudaFuncAttributeMaxDynamicSharedMemorySize, B.smem));
-        for (int e = 0; e < 2; e++) CK(cudaFuncSetAttribute(eval_fn(B.T, B.S, e), cudaFuncAttributeMaxDynamicSharedMemorySize, B.smem));
+        if (!fns[0] || !fns[1]) return fail("no kernel for bucket (kind %d, T=%d, S=%d)", B.kind, B.T, B.S);
+        for (int f = 0; f < 2; f++) CK(cudaFuncSetAttribute(fns[f], cudaFuncAttributeMaxDynamicSharedMemorySize, B.smem));
+        for (int e = 0; e < 2; e++) {
+            void* ef = B.kind ? eval_warp_fn(B.apl, e) : eval_fn(B.T, B.S, e);
+            CK(cudaFuncSetAttribute(ef, cudaFuncAttributeMaxDynamicSharedMemorySize, B.smem));
+        }
         int occ = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, B.T, B.smem));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fns[0], B.T, B.smem));
         if (occ < 1) return fail("kernel cannot be resident (T=%d smem=%d)", B.T, B.smem);
-        B.grid = std::min((int)B.sys.size(), occ * nsm);
+        const int per_block = B.kind ? 4 : 1;
+        const int nblk = ((int)B.sys.size() + per_block - 1) / per_block;
+        B.grid = std::min(nblk, occ * nsm);
         if (B.queue.ensure(B.sys.size())) return -1;
         CK(cudaMemcpy(B.queue.p, B.sys.data(), B.sys.size() * sizeof(int), cudaMemcpyHostToDevice));
         W.buckets.push_back(std::move(B));
@@ -245,8 +271,9 @@ int mmff_set_params(int flags, const int* nPBC, double Rcut, double alphaMorse, 
 }
 
 int mmff_set_fire(double dt_max, double dt_min, double damp_max, double finc, double fdec, double falpha,
-                  int minLastNeg, double cv_kill, double Flim) {
-    double f[9] = {dt_max, dt_min, damp_max, finc, fdec, falpha, (double)minLastNeg, cv_kill, Flim};
+                  int minLastNeg, double cv_kill, double Flim, int variant) {
+    if (variant != 0 && variant != 1) return fail("FIRE variant must be 0 or 1");
+    double f[10] = {dt_max, dt_min, damp_max, finc, fdec, falpha, (double)minLastNeg, cv_kill, Flim, (double)variant};
     memcpy(W.fire, f, sizeof f);
     return 0;
 }
@@ -448,12 +475,13 @@ int mmff_eval(int with_energy) {
     Params P = make_params(true, 0, 0.0, 0);
     Systems Y = make_systems();
     for (auto& B : W.buckets) {
-        void* fn = eval_fn(B.T, B.S, with_energy != 0);
+        void* fn = B.kind ? eval_warp_fn(B.apl, with_energy != 0) : eval_fn(B.T, B.S, with_energy != 0);
         const int* q = B.queue.p;
         int nq = (int)B.sys.size();
         int mna = B.maxNA, mnn = B.maxNN;
         void* args[] = {&P, &Y, &q, &nq, &mna, &mnn};
-        CK(cudaLaunchKernel(fn, dim3(nq), dim3(B.T), args, B.smem, W.stream));
+        const int nblk = B.kind ? (nq + 3) / 4 : nq;
+        CK(cudaLaunchKernel(fn, dim3(nblk), dim3(B.T), args, B.smem, W.stream));
     }
     CK(cudaGetLastError());
     return 0;
@@ -473,7 +501,7 @@ int mmff_relax(int nstep_max, double Fconv, int conv_mode) {
         Bucket& B = W.buckets[b];
         cudaStream_t st = W.bstreams[b];
         CK(cudaStreamWaitEvent(st, W.evfork, 0));
-        void* fn = relax_fn(B.T, B.S, W.count);
+        void* fn = B.kind ? relax_warp_fn(B.apl, W.count) : relax_fn(B.T, B.S, W.count);
         const int* q = B.queue.p;
         int nq = (int)B.sys.size();
         int* ctr = W.d_counter.p + b;
@@ -590,7 +618,7 @@ int mmff_num_buckets(void) { return W.buckets_dirty ? -1 : (int)W.buckets.size()
 int mmff_bucket_info(int b, int* info) {
     if (b < 0 || b >= (int)W.buckets.size()) return fail("bad bucket");
     const Bucket& B = W.buckets[b];
-    info[0] = B.T; info[1] = B.S; info[2] = (int)B.sys.size(); info[3] = B.maxNA; info[4] = B.maxNN; info[5] = B.smem; info[6] = B.grid;
+    info[0] = B.T; info[1] = B.kind ? -B.apl : B.S; info[2] = (int)B.sys.size(); info[3] = B.maxNA; info[4] = B.maxNN; info[5] = B.smem; info[6] = B.grid;
     return 0;
 }
 

@@ -38,6 +38,7 @@ class FireParams:
     minLastNeg: int = 3
     cv_kill: float = 0.0
     Flim: float = -1.0
+    variant: int = 0       # 0: run_no_omp velocity kick; 1: Bitzek et al. 2006 mixing
 
 
 def _check(rc, what):
@@ -62,7 +63,7 @@ class World:
 
     def set_fire(self, F: FireParams = FireParams()):
         _check(self.lib.mmff_set_fire(F.dt_max, F.dt_min, F.damp_max, F.finc, F.fdec, F.falpha, int(F.minLastNeg),
-                                      F.cv_kill, F.Flim), "mmff_set_fire")
+                                      F.cv_kill, F.Flim, int(F.variant)), "mmff_set_fire")
 
     def set_launch(self, threads=0, pair_split=0):
         _check(self.lib.mmff_set_launch(threads, pair_split), "mmff_set_launch")

@@ -45,11 +45,16 @@ int mmff_sync(void);
 int mmff_set_params(int flags, const int* nPBC, double Rcut, double alphaMorse, double FmaxNonBonded);
 /* FIRE parameters (DynamicOpt members, cpp/common/math/DynamicOpt.h:73-95;
  * set_opt, cpp/libs_OCL/MMFFmulti_lib.cpp:141).  Flim > 0 clamps each
- * assembled force vector to |f| <= Flim (relax_multi.cl:980-983). */
+ * assembled force vector to |f| <= Flim (relax_multi.cl:980-983).
+ * variant 0: the velocity kick of MolWorld_sp3::run_no_omp, f*(dt + renorm*cf)
+ * with cf = renorm*damping (MolWorld_sp3.h:2426); variant 1: the mixing of
+ * Bitzek et al. (2006), f*(dt + cf). */
 int mmff_set_fire(double dt_max, double dt_min, double damp_max, double finc, double fdec, double falpha,
-                  int minLastNeg, double cv_kill, double Flim);
+                  int minLastNeg, double cv_kill, double Flim, int variant);
 /* Threads per CTA (64/128/256/512) and lanes per atom in the pair sum
- * (1/2/4/8); 0 = chosen per size bucket. */
+ * (1/2/4/8) of the CTA-per-system kernels; 0 = chosen per size bucket
+ * (systems of <= 64 atoms then run one per warp).  A non-zero thread count
+ * forces every system onto the CTA-per-system kernels. */
 int mmff_set_launch(int threads, int pair_split);
 
 /* ------------------------------------------------------------ substrate grid */
@@ -135,7 +140,8 @@ int mmff_get_counters(unsigned long long* out);
 double mmff_peak_fp32(void);
 double mmff_peak_l2(int mbytes);
 int mmff_num_buckets(void);
-/* info[7] = (threads, pair_split, nsys, maxNA, maxNN, smem bytes, CTAs) */
+/* info[7] = (threads, pair_split, nsys, maxNA, maxNN, smem bytes, CTAs);
+ * pair_split < 0 marks a warp-per-system bucket with -pair_split atoms per lane */
 int mmff_bucket_info(int b, int* info);
 
 /* ------------------------------------------------------------ synthetic workloads */
@@ -150,6 +156,83 @@ int mmff_gen_systems(int nsys, const int* natoms, uint64_t seed, int topo_mode, 
 /* Rock-salt (001) slab; returns the number of ions. */
 int mmff_gen_slab(double a, int ncell, int layers, double z_top, double q, const double* REQ_cation,
                   const double* REQ_anion, double* spos, double* sREQ);
+
+
+/* ============================================================================
+ * Legacy symbols: the reference library's ABI as pyBall/MMFF_multi.py binds it
+ * (argtypes at pyBall/MMFF_multi.py:99-599).  One global world of nSys
+ * replicas of one molecule with host mirrors of the device buffers, served
+ * by the CSR API above.  All compute runs on the GPU.
+ * ========================================================================== */
+
+/* libUtils.h:16-47 -- name -> host buffer registry */
+void   printBuffNames(void);
+double* getBuff(const char* name);     /* apos fapos DOFs fDOFs vDOFs pipos fpipos Es */
+float*  getfBuff(const char* name);    /* gpu_atoms gpu_aforces gpu_avel gpu_constr gpu_REQs gpu_MMpars
+                                          gpu_BLs gpu_BKs gpu_Ksp gpu_Kpp gpu_lvecs gpu_ilvecs gpu_pbcshifts */
+int*    getIBuff(const char* name);    /* ndims neighs selection gpu_neighs gpu_neighCell gpu_bkNeighs */
+
+/* cpp/libs_OCL/MMFFmulti_lib.cpp */
+void  init_buffers(void);                                                   /* :23 */
+void* init(int nSys, char* xyz_name, char* surf_name, char* smile_name, bool bMMFF, bool bEpairs, int* nPBC,
+           int* grid_nPBC, double gridStep, char* sElementTypes, char* sAtomTypes, char* sBondTypes,
+           char* sAngleTypes, double T, double gamma, int nExplore, int nRelax, double pos_kick, double vel_kick,
+           int GridFF);                                                     /* :75 */
+int   run(int nstepMax, double dt, double Fconv, int ialg, double* outE, double* outF, int iParalel);   /* :116 */
+void  MDloop(int perframe, double Ftol, int iParalel, int perVF);           /* :134 */
+void  set_opt(double dt_max, double dt_min, double damp_max, double finc, double fdec, double falpha, int minLastNeg,
+              double cvf_min, double cvf_max);                              /* :141 */
+void  sampleSurf(char* name, int n, double* rs, double* Es, double* fs, int kind, int atyp, double Q, double K,
+                 double RQ, double* pos0_, bool bSave);                     /* :168 */
+void  sampleSurf_vecs(char* name, int n, double* poss_, double* Es, double* fs_, int kind, int atyp, double Q,
+                      double K, double RQ, double* pos0_, bool bSave);      /* :210 */
+void  pack_system(int isys, bool bParams, bool bForces, bool bVel, bool blvec);   /* :253 */
+void  unpack_system(int isys, bool bForces, bool bVel);                     /* :256 */
+void  upload_sys(int isys, bool bParams, bool bForces, bool bVel, bool blvec);    /* :260 */
+void  download_sys(int isys, bool bForces, bool bVel);                      /* :263 */
+void  upload(bool bParams, bool bForces, bool bVel, bool blvec);            /* :267 */
+void  download(bool bForces, bool bVel);                                    /* :270 */
+void  change_lvec(double* lvec, bool bAdd, bool bUpdatePi);                 /* :275 */
+void  upload_pop(const char* fname);                                        /* :281 */
+void  optimizeLattice_1d(double* dlvec, int n1, int n2, int initMode, double tol);         /* :289 */
+void  optimizeLattice_2d_multi(double* dlvec, int nstesp, int initMode, double tol);       /* :294 */
+void  scan(int nconf, double* poss, double* rots, double* Es, double* aforces, double* aposs, bool omp, bool bRelax,
+           int niter_max, double dt, double Fconv, double Flim);            /* :305 */
+void  setSwitches_multi(int CheckInvariants, int PBC, int NonBonded, int MMFF, int Angles, int PiSigma, int PiPiI,
+                        int dovdW, int bSaveToDatabase);                    /* :316 */
+
+/* cpp/common/molecular/libMMFF.h */
+void  setVerbosity(int verbosity_, int idebug_);                            /* :15 */
+void  insertSMILES(char* s);                                                /* :25 */
+bool  checkInvariants(double maxVcog, double maxFcog, double maxTg);        /* :52 */
+void  setOptLog(int n, double* cos, double* f, double* v, double* dt, double* damp);
+bool  setTrjName(const char* trj_fname_, int savePerNsteps_);               /* :53 */
+int   saveXYZ(const char* fname, const char* comment, int imod);            /* :55 */
+const char* getTypeName(int ia, bool fromFF);                               /* :112 */
+double eval(void);                                                          /* :98 */
+void  addDistConstrain(int i0, int i1, double lmin, double lmax, double kmin, double kmax, double flim, double* shift,
+                       bool bOldIndex);                                     /* :41 */
+void  addAngConstrain(int i0, int i1, int i2, double ang0, double k);       /* :46 */
+void  shift_atoms_ax(int n, int* selection, double* d);                     /* :122 */
+void  shift_atoms(int n, int* selection, int ia0, int ia1, double l);       /* :124 */
+void  rotate_atoms_ax(int n, int* selection, double* p0, double* ax, double phi);         /* :123 */
+void  rotate_atoms(int n, int* selection, int ia0, int iax0, int iax1, double phi);       /* :125 */
+void  scanTranslation_ax(int n, int* selection, double* vec, int nstep, double* Es, const char* trjName,
+                         bool bAddjustCaps);                                /* :134 */
+void  scanTranslation(int n, int* selection, int ia0, int ia1, double l, int nstep, double* Es, const char* trjName,
+                      bool bAddjustCaps);                                   /* :138 */
+void  scanRotation_ax(int n, int* selection, double* p0, double* ax, double phi, int nstep, double* Es,
+                      const char* trjName);                                 /* :141 */
+void  scanRotation(int n, int* selection, int ia0, int iax0, int iax1, double phi, int nstep, double* Es,
+                   const char* trjName);                                    /* :147 */
+void  sample_DistConstr(double lmin, double lmax, double kmin, double kmax, double flim, int n, double* xs, double* Es,
+                        double* Fs);                                        /* :426 */
+void  sample_evalPiAling(double k, double ang0, double r1, double r2, int n, double* angles, double* Es, double* Fs);   /* :439 */
+void  sample_evalAngleCos(double k, double ang0, double r1, double r2, int n, double* angles, double* Es, double* Fs);  /* :451 */
+void  sample_evalAngleCosHalf(double k, double ang0, double r1, double r2, int n, double* angles, double* Es,
+                              double* Fs);                                  /* :464 */
+void  sampleNonBond(int n, double* rs, double* Es, double* fs, int kind, double* REQi_, double* REQj_, double K,
+                    double Rdamp);                                          /* :477 */
 
 #ifdef __cplusplus
 }

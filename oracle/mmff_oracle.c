@@ -582,7 +582,7 @@ void orc_relax(int nsys, const int* natoms, const int* nnode,
             }
             /* move_atom_FIRE(i, (float)dt, Flim, cv, renorm_vf*cf) */
             const double dtf = (double)(float)dt;
-            const double cfm = renorm_vf * cf;
+            const double cfm = (F->variant == 1) ? cf : renorm_vf * cf;
             for (int i = 0; i < nv; i++) {
                 v3 f = ld3(S.force + 3 * i), vi = ld3(v + 3 * i), pi = ld3(p + 3 * i);
                 const int bPi = i >= S.natoms;

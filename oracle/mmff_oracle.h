@@ -63,6 +63,9 @@ typedef struct {
 typedef struct {
     double dt_max, dt_min, damp_max, finc, fdec, falpha, cv_kill;
     int    minLastNeg;
+    int    variant; /* 0: run_no_omp mixing, velocity gets f*(dt + renorm_vf*cf)
+                       (MolWorld_sp3.h:2426, cf already = renorm_vf*damping);
+                       1: Bitzek et al. 2006 mixing, f*(dt + cf) */
     double Flim;   /* >0: per-vector force clamp |f|<=Flim after assembly, as in
                       relax_multi.cl:980-983 (updateAtomsMMFFf4); <=0: none, as
                       run_no_omp (MolWorld_sp3.h:2426 passes Flim=1e4, unused) */

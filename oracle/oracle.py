@@ -34,7 +34,8 @@ class ORCParams(ctypes.Structure):
 class ORCFire(ctypes.Structure):
     _fields_ = [("dt_max", ctypes.c_double), ("dt_min", ctypes.c_double), ("damp_max", ctypes.c_double),
                 ("finc", ctypes.c_double), ("fdec", ctypes.c_double), ("falpha", ctypes.c_double),
-                ("cv_kill", ctypes.c_double), ("minLastNeg", ctypes.c_int), ("Flim", ctypes.c_double)]
+                ("cv_kill", ctypes.c_double), ("minLastNeg", ctypes.c_int), ("variant", ctypes.c_int),
+                ("Flim", ctypes.c_double)]
 
 
 def _p(a):
@@ -109,12 +110,13 @@ def make_params(grid=None, flags=DEFAULT_FLAGS, npbc=(1, 1, 0), Rcut=-1.0, Ron=-
 
 
 def make_fire(dt_max=0.1, dt_min=0.01, damp_max=0.1, finc=1.1, fdec=0.5, falpha=0.8, minLastNeg=3,
-              cv_kill=0.0, Flim=-1.0) -> ORCFire:
+              cv_kill=0.0, Flim=-1.0, variant=0) -> ORCFire:
     """Defaults = DynamicOpt after setTimeSteps(0.1) / initOpt (DynamicOpt.h:73-95, 199-205)."""
     F = ORCFire()
     F.dt_max, F.dt_min, F.damp_max, F.finc, F.fdec, F.falpha, F.cv_kill = dt_max, dt_min, damp_max, finc, fdec, falpha, cv_kill
     F.minLastNeg = minLastNeg
     F.Flim = Flim
+    F.variant = variant
     return F
 
 
