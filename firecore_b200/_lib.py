@@ -56,6 +56,12 @@ def _declare(lib):
         "mmff_relax": [c_int, c_double, c_int], "mmff_get_forces": [c_void], "mmff_get_energies": [c_void],
         "mmff_get_state": [c_void] * 6, "mmff_timer_start": [], "mmff_num_buckets": [],
         "mmff_bucket_info": [c_int, c_void], "mmff_set_counting": [c_int], "mmff_get_counters": [c_void],
+        "mmff_mlp_set_params": [c_void, c_void, c_void, c_double], "mmff_mlp_get_params": [c_void],
+        "mmff_mlp_grad": [c_int, c_void, c_void, c_void, c_void], "mmff_mlp_adamw": [c_void, c_double, c_double],
+        "mmff_mlp_infer": [c_int, c_void, c_void], "mmff_mlp_set_data": [c_int, c_void, c_void],
+        "mmff_mlp_train": [c_int, c_int, c_double, c_double, c_void], "mmff_mlp_set_elements": [c_void],
+        "mmff_mlp_features": [c_double, c_void], "mmff_mlp_warmstart": [c_int, c_double, c_void],
+        "mmff_mlp_plan": [c_void], "mmff_mlp_layout": [c_void],
     }
     for name, args in sig.items():
         f = getattr(lib, name)
@@ -67,3 +73,7 @@ def _declare(lib):
     lib.mmff_peak_fp32.restype = c_double
     lib.mmff_peak_l2.argtypes = [c_int]
     lib.mmff_peak_l2.restype = c_double
+    lib.mmff_mlp_smem_desc.argtypes = [ctypes.c_uint, ctypes.c_uint, ctypes.c_uint]
+    lib.mmff_mlp_smem_desc.restype = ctypes.c_ulonglong
+    lib.mmff_mlp_instr_desc.argtypes = [c_int, c_int, c_int]
+    lib.mmff_mlp_instr_desc.restype = ctypes.c_uint

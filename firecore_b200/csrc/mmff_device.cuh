@@ -296,6 +296,51 @@ __device__ __forceinline__ float4 grid_slice(const float4* __restrict__ G, int n
     return make_float4(dxa * ez, bxa * ex, bxa * ey, bxa * ez);
 }
 
+// B-spline GridFF force + energy of one atom, the whole 4x4x4 stencil in this
+// lane (Bspline::fe3d_pbc_comb3, Bspline.h:742-809; the same index and basis
+// arithmetic as grid_slice)
+__device__ __forceinline__ float4 grid_atom(const Params& P, float3 u, float4 PLQ) {
+    const int nx = P.gn[0], ny = P.gn[1], nz = P.gn[2];
+    const float4* __restrict__ G = P.grid;
+    int ix = (int)u.x, iy = (int)u.y, iz = (int)u.z;
+    if (u.x < 0.f) ix--;
+    if (u.y < 0.f) iy--;
+    const float tx = u.x - (float)ix, ty = u.y - (float)iy, tz = u.z - (float)iz;
+    iz = min(max(iz, 3), nz - 5);
+    ix = ix - 1; ix %= nx; if (ix < 0) ix += nx;
+    iy = iy - 1; iy %= ny; if (iy < 0) iy += ny;
+    const float4 bz = bs_basis(tz), dz = bs_dbasis(tz);
+    const float4 by = bs_basis(ty), dy = bs_dbasis(ty);
+    const float4 bx = bs_basis(tx), dx = bs_dbasis(tx);
+    float Fx = 0.f, Fy = 0.f, Fz = 0.f, E = 0.f;
+#pragma unroll 1
+    for (int a = 0; a < 4; a++) {
+        int xa = ix + a; if (xa >= nx) xa -= nx;
+        float ex = 0.f, ey = 0.f, ez = 0.f;
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+            int yb = iy + b; if (yb >= ny) yb -= ny;
+            const float4* col = G + ((size_t)(xa * ny + yb) * nz + (iz - 1));
+            const float4 c0 = __ldg(col), c1 = __ldg(col + 1), c2 = __ldg(col + 2), c3 = __ldg(col + 3);
+            const float cs0 = fmaf(PLQ.x, c0.x, fmaf(PLQ.y, c0.y, PLQ.z * c0.z));
+            const float cs1 = fmaf(PLQ.x, c1.x, fmaf(PLQ.y, c1.y, PLQ.z * c1.z));
+            const float cs2 = fmaf(PLQ.x, c2.x, fmaf(PLQ.y, c2.y, PLQ.z * c2.z));
+            const float cs3 = fmaf(PLQ.x, c3.x, fmaf(PLQ.y, c3.y, PLQ.z * c3.z));
+            const float v = fmaf(bz.x, cs0, fmaf(bz.y, cs1, fmaf(bz.z, cs2, bz.w * cs3)));
+            const float d = fmaf(dz.x, cs0, fmaf(dz.y, cs1, fmaf(dz.z, cs2, dz.w * cs3)));
+            const float byb = comp(by, b), dyb = comp(dy, b);
+            ex = fmaf(v, dyb, ex);
+            ey = fmaf(d, byb, ey);
+            ez = fmaf(v, byb, ez);
+        }
+        const float bxa = (a == 0) ? bx.x : (a == 1) ? bx.y : (a == 2) ? bx.z : bx.w;
+        const float dxa = (a == 0) ? dx.x : (a == 1) ? dx.y : (a == 2) ? dx.z : dx.w;
+        Fx = fmaf(dxa, ez, Fx); Fy = fmaf(bxa, ex, Fy); Fz = fmaf(bxa, ey, Fz); E = fmaf(bxa, ez, E);
+    }
+    return make_float4(Fx * P.gmi[0], Fy * P.gmi[1], Fz * P.gmi[2], E);
+}
+
+
 // ---- shared-memory carve-up of one system (byte offsets)
 struct SmemLayout {
     int maxNA, maxNN, maxNV, nwarps;

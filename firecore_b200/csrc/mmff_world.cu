@@ -18,6 +18,7 @@
 #include "MMFFmulti_lib.h"
 #include "mmff_device.cuh"
 #include "mmff_host.h"
+#include "mmff_world.h"
 
 namespace mmff {
 // kernels (mmff_relax.cu, mmff_grid.cu)
@@ -241,6 +242,24 @@ template <class X> int upload(DBuf<X>& d, const std::vector<X>& h) {
 }  // namespace
 
 void mmff_set_error(const char* msg) { g_err = msg; }
+
+namespace mmff {
+
+cudaStream_t world_stream() { return ensure_ready() ? nullptr : W.stream; }
+
+int world_view(WorldView* v) {
+    if (ensure_ready()) return -1;
+    if (!W.nsys) return fail("no systems uploaded");
+    v->P = make_params(true, 0, 0.0, 0);
+    v->Y = make_systems();
+    v->stream = W.stream;
+    v->nsys = W.nsys; v->NA = W.NA; v->NV = W.NV;
+    v->desc = W.desc.data();
+    for (int k = 0; k < 3; k++) v->gpos0[k] = W.gpos0[k];
+    return 0;
+}
+
+}  // namespace mmff
 
 // ============================================================================ C-ABI
 extern "C" {

@@ -234,6 +234,51 @@ void  sample_evalAngleCosHalf(double k, double ang0, double r1, double r2, int n
 void  sampleNonBond(int n, double* rs, double* Es, double* fs, int kind, double* REQi_, double* REQj_, double K,
                     double Rdamp);                                          /* :477 */
 
+/* ------------------------------------------------------------ learned warm-start proposal
+ * No counterpart in FireCore (its relaxers are plain FIRE,
+ * MolWorld_sp3.h:2261-2490); the network is this library's addition: per-atom
+ * descriptors (32 nearest neighbours within 5 A: 16 Gaussian radial bins,
+ * sigma 0.3 A, x 4 element channels H C N O; height above the slab; GridFF
+ * force) -> 68 -> 128 -> 128 -> 3 SiLU MLP predicting a displacement toward the
+ * minimum.  BF16 weights and activations, FP32 accumulation on the tensor
+ * cores (tcgen05).  Flat FP32 parameter vector: W1 [128][80] (inputs >= 68
+ * zero), b1 [128], W2 [128][128], b2 [128], W3 [16][128] (rows >= 3 zero),
+ * b3 [16] (see mmff_mlp_layout for the offsets).  Targets and outputs are in
+ * A; the network works in units of out_scale. */
+/* Parameters (flat vector), feature standardisation (mean, std > 0 per
+ * feature) and output scale [A]; resets the AdamW moments and step count. */
+int mmff_mlp_set_params(const float* prm, const float* feat_mean, const float* feat_std, double out_scale);
+int mmff_mlp_get_params(float* prm);
+/* Gradient sums of the mean squared displacement error over n rows of raw
+ * features [n][68] and targets [n][3] (no update); loss = sum |y - t|^2 / n. */
+int mmff_mlp_grad(int n, const float* feat, const float* target, float* grad_out, double* loss_out);
+/* One AdamW step (beta 0.9/0.999, eps 1e-8, decoupled decay wd on W1..W3)
+ * with the given flat FP32 gradients (NULL: the last computed ones). */
+int mmff_mlp_adamw(const float* grad, double lr, double wd);
+/* Network displacement [n][3] (A) for raw features [n][68]. */
+int mmff_mlp_infer(int n, const float* feat, float* out);
+/* Device-resident training set (rows in the order given) and nsteps AdamW
+ * steps over consecutive batches of batch_tiles x 128 rows; per-step losses
+ * to loss_out [nsteps] (nullable). */
+int mmff_mlp_set_data(int n, const float* feat, const float* target);
+int mmff_mlp_train(int nsteps, int batch_tiles, double lr, double wd, double* loss_out);
+/* Element channel per atom of the uploaded systems [sum natoms] (0 H, 1 C,
+ * 2 N, 3 O; larger values use channel 3). */
+int mmff_mlp_set_elements(const int* elem);
+/* Raw descriptors [sum natoms][68] of the current positions; z_top = slab top [A]. */
+int mmff_mlp_features(double z_top, float* out);
+/* nsteps learned moves on every system: descriptors -> network -> move the
+ * atoms -> keep the move only where the total energy dropped; accepted
+ * [nsys] (nullable) counts the kept moves.  Velocities and FIRE state are
+ * left as they are. */
+int mmff_mlp_warmstart(int nsteps, double z_top, int* accepted);
+/* Introspection for host-side checks: the tcgen05 product plan (14 ints per
+ * product; returns the count), sizes/offsets, and the descriptor encoders. */
+int mmff_mlp_plan(int* ops);
+int mmff_mlp_layout(int* out);
+unsigned long long mmff_mlp_smem_desc(unsigned addr, unsigned lbo, unsigned sbo);
+unsigned mmff_mlp_instr_desc(int n, int a_mn, int b_mn);
+
 #ifdef __cplusplus
 }
 #endif
