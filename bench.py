@@ -41,17 +41,32 @@ RCUT = 10.0
 FLIM = 10.0
 PAIR_FLOPS = 32          # algorithmic FP32 flops per pair-image (both directions counted)
 GRID_BYTES = 1024        # 64 float4 gathers per atom B-spline sample
+# DRAM bytes (read + write) per system-step of the warp-engine relax kernel,
+# from the ncu capture in profiles/relax_warp_kernel_4096x60.md (86.5 MB over
+# 4096 systems x 200 steps); scaled by the system-steps of a launch
+DRAM_BYTES_PER_SYSTEM_STEP = 105.6
 
 
 def env_rank():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
-def workload(rank, nsys):
+def workload(rank, nsys, kind="replicas"):
     from firecore_b200 import systems as S
     sub = S.make_slab()                      # 226 x 226 x 200, nPBC_coul (25,25,0)
-    batch = S.config_replicas(seed=1 + 7919 * rank, nrep=nsys)
+    if kind == "uneven":
+        batch = S.config_uneven(seed=2 + 7919 * rank, nsys=nsys)
+    else:
+        batch = S.config_replicas(seed=1 + 7919 * rank, nrep=nsys)
     return sub, batch
+
+
+def workload_name(args):
+    if args.workload == "uneven":
+        return (f"{args.nsys} distinct molecules, 20-400 atoms log-uniform (CSR, size buckets, per-bucket work "
+                f"queues) on NaCl slab, GridFF 226x226x200, Rcut {RCUT} A, Fmax<{FCONV}, <= {MAXSTEPS} FIRE steps")
+    return (f"{args.nsys} replicas x 60-atom molecule on NaCl slab, GridFF 226x226x200, "
+            f"Rcut {RCUT} A, Fmax<{FCONV}, <= {MAXSTEPS} FIRE steps")
 
 
 def cpu_info():
@@ -127,7 +142,7 @@ def run_ours(args):
     from firecore_b200 import _lib
     from firecore_b200.world import DEFAULT_FLAGS, FireParams, World
     lib = _lib.load()
-    sub, batch = workload(rank, args.nsys)
+    sub, batch = workload(rank, args.nsys, args.workload)
     w = World(lrank)
     t0 = time.perf_counter()
     C = w.grid_build(sub, return_coefs=True)
@@ -146,6 +161,7 @@ def run_ours(args):
     pair_images, grid_samples, force_evals = int(cnt[0]), int(cnt[1]), int(cnt[2])
     lib.mmff_set_counting(0)
     st0 = w.state()
+    attr_t, attr_pairs, attr_grid = term_attribution(w, lib)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")   # > 126 MB L2
 
     def one_step():
@@ -212,6 +228,10 @@ def run_ours(args):
     t_launch = t_dev / args.steps
     achieved_tf = PAIR_FLOPS * pair_images / t_launch / 1e12
     grid_gbs = GRID_BYTES * grid_samples / t_launch / 1e9
+    t_pair = (attr_t["all"] - attr_t["no_pairs"]) / 1e3
+    t_grid = (attr_t["all"] - attr_t["no_grid"]) / 1e3
+    pair_tf = PAIR_FLOPS * attr_pairs / t_pair / 1e12 if t_pair > 0 else None
+    grid_term_gbs = GRID_BYTES * attr_grid / t_grid / 1e9 if t_grid > 0 else None
     out = None
     if rank == 0:
         cpu = cpu_baseline(batch, sub, C, args) if not args.no_cpu else None
@@ -221,8 +241,7 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": wsize, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 forces / f64 FIRE reductions", "data": "synthetic (seeded generator)",
-            "config": {"workload": f"{args.nsys} replicas x 60-atom molecule on NaCl slab, GridFF 226x226x200, "
-                                   f"Rcut {RCUT} A, Fmax<{FCONV}, <= {MAXSTEPS} FIRE steps",
+            "config": {"workload": workload_name(args),
                        "systems_per_gpu": args.nsys, "l2": "flushed (256 MB write) before every step",
                        "parallelism": f"replicas x{wsize}"},
             "converged_per_step": conv / args.steps, "nan_per_step": nans / args.steps,
@@ -231,12 +250,22 @@ def run_ours(args):
             "grid_build_s": grid_build_s, "wall_s_timed": t_wall,
             "gpu_launches": args.steps * len(w.buckets()),
             "roofline": {"bound": "fp32", "achieved": achieved_tf, "peak": fp32_peak, "unit": "TFLOP/s",
-                         "frac": achieved_tf / fp32_peak if fp32_peak > 0 else None, "traffic": None,
+                         "frac": achieved_tf / fp32_peak if fp32_peak > 0 else None,
+                         "traffic": DRAM_BYTES_PER_SYSTEM_STEP * force_evals,
                          "peak_source": "measured FFMA microbenchmark (mmff_peak_fp32) on this GPU",
                          "work": f"{PAIR_FLOPS} flop x {pair_images} pair-images per launch",
                          "grid_l2": {"achieved": grid_gbs, "peak": l2_peak, "unit": "GB/s",
                                      "frac": grid_gbs / l2_peak if l2_peak > 0 else None,
-                                     "work": f"{GRID_BYTES} B x {grid_samples} atom samples per launch"}},
+                                     "work": f"{GRID_BYTES} B x {grid_samples} atom samples per launch"},
+                         "pair_term": {"achieved": pair_tf, "peak": fp32_peak, "unit": "TFLOP/s",
+                                       "frac": pair_tf / fp32_peak if (pair_tf and fp32_peak > 0) else None,
+                                       "time_ms": 1e3 * t_pair, "work": f"{PAIR_FLOPS} flop x {attr_pairs} pair-images",
+                                       "method": "200-step relax of the batch with all terms minus without the pair term"},
+                         "grid_term": {"achieved": grid_term_gbs, "peak": l2_peak, "unit": "GB/s",
+                                       "frac": grid_term_gbs / l2_peak if (grid_term_gbs and l2_peak > 0) else None,
+                                       "time_ms": 1e3 * t_grid,
+                                       "method": "200-step relax with all terms minus without GridFF"},
+                         "term_times_ms": attr_t},
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
             "buckets": w.buckets(),
         }
@@ -247,12 +276,54 @@ def run_ours(args):
     return out
 
 
+def term_attribution(w, lib, nsteps=200):
+    """Device time of each force term inside the fused relax kernel: the same
+    fixed-length relaxation (Fmax < 0 never converges, so every system runs
+    nsteps steps) with all terms, and with one term switched off.  Returns
+    times [ms] and the pair-images / grid samples of the full run."""
+    from firecore_b200.world import ANGLES, BONDS, DEFAULT_FLAGS, GRID, NONBONDED, PIPI, PISIGMA, SUB_ANGLE_NB
+    # without the pair term the 1-3 subtraction of the angle terms must go too,
+    # or the molecules collapse and retire as non-finite
+    variants = {"all": DEFAULT_FLAGS, "no_pairs": DEFAULT_FLAGS & ~(NONBONDED | SUB_ANGLE_NB),
+                "no_grid": DEFAULT_FLAGS & ~GRID, "no_bonded": DEFAULT_FLAGS & ~(BONDS | ANGLES | PIPI | PISIGMA)}
+    times, nan = {}, {}
+    for name, fl in variants.items():
+        w.set_params(flags=fl, npbc=(1, 1, 0), Rcut=RCUT)
+        best = 1e30
+        for _ in range(3):
+            w.restore()
+            w.sync()
+            w.timer_start()
+            w.relax(nsteps, 0.0, 1, sync=False)
+            best = min(best, w.timer_stop())
+        times[name] = best
+        st = np.zeros(w.batch.nsys, np.int32)
+        lib.mmff_get_state(None, None, None, _lib_ptr(st), None, None)
+        nan[name] = int((st == -1).sum())
+    w.set_params(flags=DEFAULT_FLAGS, npbc=(1, 1, 0), Rcut=RCUT)
+    lib.mmff_set_counting(1)
+    w.restore(); w.relax(nsteps, 0.0, 1)
+    cnt = (np.ctypeslib.ctypes.c_ulonglong * 3)()
+    lib.mmff_get_counters(np.ctypeslib.ctypes.cast(cnt, np.ctypeslib.ctypes.c_void_p))
+    lib.mmff_set_counting(0)
+    w.restore()
+    times["retired_nonfinite"] = nan
+    return times, int(cnt[0]), int(cnt[1])
+
+
+def _lib_ptr(a):
+    from firecore_b200 import _lib
+    return _lib.ptr(a)
+
+
 def cpu_baseline(batch, sub, C, args):
     """The FP64 oracle (OpenMP over systems) on a bounded sample of the same
     workload, same parameters (10 A cutoff, force clamp, Fmax criterion)."""
     from oracle import oracle as O
     model, ncores = cpu_info()
-    nsample = int(min(batch.nsys, max(16, 4 * ncores), 256))
+    nsample = int(min(batch.nsys, max(64, 32 * ncores), 1024))
+    if args.workload == "uneven":             # up to 400 atoms: ~25x the pair work of a 60-atom system
+        nsample = int(min(batch.nsys, max(16, 2 * ncores)))
     sb = batch.subset(range(nsample))
     P = O.make_params(sub.grid, npbc=(1, 1, 0), Rcut=RCUT)
     F = O.make_fire(Flim=FLIM)
@@ -262,6 +333,104 @@ def cpu_baseline(batch, sub, C, args):
     conv = int((r["converged"] == 1).sum())
     return {"value": conv / dt, "unit": UNIT, "cores": ncores, "kind": "port",
             "sample": f"{nsample} of the systems, full relaxation each ({conv} converged, {dt:.1f} s), CPU: {model}"}
+
+
+# --------------------------------------------------------------------------- learned vs plain
+def run_learned(args):
+    """Learned warm start + batched FIRE against plain batched FIRE on the
+    same fresh uneven systems.  Training set: descriptors at FIRE steps 0, 25
+    and 100 of the plain relaxer on separately seeded systems, targets = the
+    displacement to the relaxed geometry (converged systems only); the network
+    is trained on the GPU (tcgen05 forward/backward + AdamW).  Production: 2
+    energy-gated learned moves per system, then plain FIRE to Fmax < 1e-4."""
+    import torch
+    from firecore_b200 import learned as L
+    from firecore_b200 import systems as S
+    from firecore_b200.world import DEFAULT_FLAGS, FireParams, World
+    from oracle import oracle as O
+    torch.cuda.set_device(0)
+    sub = S.make_slab()
+    w = World(0)
+    C = w.grid_build(sub, return_coefs=True)
+    w.set_params(flags=DEFAULT_FLAGS, npbc=(1, 1, 0), Rcut=RCUT)
+    w.set_fire(FireParams(Flim=FLIM))
+    w.set_graph(True)
+    prop = L.Proposal()
+    # training data from the plain relaxer
+    t0 = time.perf_counter()
+    train = S.config_uneven(seed=1001, nsys=args.train_sys)
+    w.upload(train)
+    F, T = L.trajectory_dataset(w, prop, train, snapshots=(0, 25, 100), nstep_max=MAXSTEPS, Fconv=FCONV)
+    data_s = time.perf_counter() - t0
+    rng = np.random.default_rng(0)
+    perm = rng.permutation(len(F))
+    scale = float(np.sqrt((T ** 2).mean()))
+    prop.set_params(L.init_params(0), F.mean(0), F.std(0) + 1e-6, scale)
+    prop.set_data(F[perm], T[perm])
+    w.sync(); w.timer_start()
+    losses = prop.train(args.train_steps, batch_tiles=512, lr=1e-3, wd=0.01)
+    train_ms = w.timer_stop()
+    # production systems, both arms on the same inputs
+    prod = S.config_uneven(seed=2002, nsys=args.nsys)
+    w.upload(prod)
+    prop.set_elements(prod.elements)
+
+    def arm(learned):
+        w.restore()
+        w.sync()
+        w.timer_start()
+        acc = prop.warmstart(prod.nsys, 2) if learned else None
+        w.relax(MAXSTEPS, FCONV, 1, sync=False)
+        ms = w.timer_stop()
+        st = w.state()
+        _, E = w.eval()
+        return ms, st, E, acc
+
+    res = {}
+    for name, lrn in (("plain", False), ("learned", True)):
+        for _ in range(args.warmup):
+            arm(lrn)
+        tot_ms, conv = 0.0, 0
+        for _ in range(args.steps):
+            ms, st, E, acc = arm(lrn)
+            tot_ms += ms
+            conv += int((st["status"] == 1).sum())
+        res[name] = dict(ms=tot_ms / args.steps, conv=conv / args.steps, st=st, E=E, acc=acc)
+    p, l = res["plain"], res["learned"]
+    both = (p["st"]["status"] == 1) & (l["st"]["status"] == 1)
+    na = prod.natoms.astype(np.float64)
+    dE = (l["E"][:, 3] - p["E"][:, 3]) / na
+    # FP32 device energies of the final geometries against the FP64 oracle (small subset)
+    idx = [int(i) for i in np.where(l["st"]["status"] == 1)[0][:16]]
+    sb = prod.subset(idx)
+    a, _, v = prod.offsets()
+    pos_sub = np.concatenate([l["st"]["pos"][v[i]:v[i + 1]] for i in idx]) if idx else None
+    ora_err = None
+    if idx:
+        _, Eo = O.eval_forces(sb, O.make_params(sub.grid, npbc=(1, 1, 0), Rcut=RCUT), C, pos=pos_sub)
+        ora_err = float(np.max(np.abs(Eo[:, 3] - l["E"][idx, 3]) / na[idx]))
+    vp = p["conv"] / (p["ms"] / 1e3); vl = l["conv"] / (l["ms"] / 1e3)
+    med = lambda r: float(np.median(r["st"]["nsteps"][r["st"]["status"] == 1])) if (r["st"]["status"] == 1).any() else None
+    print(json.dumps({
+        "metric": "relaxed systems/s to Fmax<1e-4 eV/A on 1 B200: learned+batched vs plain FIRE", "value": vl,
+        "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": l["ms"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 forces / f64 FIRE reductions; bf16 network, f32 accumulation", "data": "synthetic (seeded generator)",
+        "config": {"workload": f"{args.nsys} fresh molecules, 20-400 atoms log-uniform, 2 energy-gated learned moves "
+                               f"then FIRE to Fmax<{FCONV} (<= {MAXSTEPS} steps); network trained on "
+                               f"{args.train_sys} separately seeded systems"},
+        "plain": {"value": vp, "ms_per_step": p["ms"], "converged": p["conv"], "median_steps": med(p)},
+        "learned": {"value": vl, "ms_per_step": l["ms"], "converged": l["conv"], "median_steps": med(l),
+                    "moves_kept_per_system": float(np.mean(l["acc"])) if l["acc"] is not None else None},
+        "speedup_learned_over_plain": vl / vp if vp > 0 else None,
+        "final_energy_learned_minus_plain_eV_per_atom": {
+            "median": float(np.median(dE[both])) if both.any() else None,
+            "p99_abs": float(np.quantile(np.abs(dE[both]), 0.99)) if both.any() else None},
+        "final_energy_vs_fp64_oracle_max_eV_per_atom": ora_err,
+        "training": {"rows": int(len(F)), "steps": args.train_steps, "batch_atoms": 512 * 128,
+                     "first_loss": float(losses[0]), "last_loss": float(np.mean(losses[-20:])),
+                     "train_ms": train_ms, "data_generation_s": data_s},
+    }))
 
 
 # --------------------------------------------------------------------------- reference arm
@@ -353,14 +522,21 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--nsys", type=int, default=4096)
+    ap.add_argument("--nsys", type=int, default=None, help="systems per GPU (default 4096; 16384 with --workload learned)")
+    ap.add_argument("--workload", default="replicas", choices=["replicas", "uneven", "learned"])
+    ap.add_argument("--train-sys", type=int, default=1024, help="--workload learned: systems whose trajectories train the network")
+    ap.add_argument("--train-steps", type=int, default=2000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--maxsteps", type=int, default=MAXSTEPS, help="FIRE step limit per system (profiling runs use fewer)")
     args = ap.parse_args()
     MAXSTEPS = args.maxsteps
+    if args.nsys is None:
+        args.nsys = 16384 if args.workload == "learned" else 4096
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "learned":
+        run_learned(args)
     else:
         run_ours(args)
 

@@ -62,6 +62,8 @@ def _declare(lib):
         "mmff_mlp_train": [c_int, c_int, c_double, c_double, c_void], "mmff_mlp_set_elements": [c_void],
         "mmff_mlp_features": [c_double, c_void], "mmff_mlp_warmstart": [c_int, c_double, c_void],
         "mmff_mlp_plan": [c_void], "mmff_mlp_layout": [c_void],
+        "mmff_set_graph": [c_int], "mmff_autotune": [c_int, c_int, c_void, c_int],
+        "mmff_get_tuning": [c_int, c_void], "mmff_set_tuning": [c_int, c_int, c_int, c_int, c_int],
     }
     for name, args in sig.items():
         f = getattr(lib, name)

@@ -16,7 +16,8 @@
 //   dW2 += dZ2^T H1 ; db2 += dZ2^T 1 ; dH1 = dZ2 W2 -> dZ1 = dH1 * silu'(Z1)
 //   dW1 += dZ1^T X  ; db1 += dZ1^T 1
 // Weight gradients accumulate in TMEM columns 256..511 over all tiles of the
-// CTA and are added to global memory once at the end.  Shared-memory layout
+// CTA and are stored once at the end as this CTA's partial sums; a second
+// kernel adds the partials of all CTAs in a fixed order (no atomics).  Shared-memory layout
 // and the descriptor of every product: mmff_umma.h.  Inference runs the first
 // three products only.
 #include <cuda_bf16.h>
@@ -148,8 +149,8 @@ struct NetArgs {
     const float4* T;         // targets (x, y, z, weight) [ntile*128]; training only
     const uint4* Wp;         // packed bf16 weights
     const float* prm;        // flat FP32 parameters (biases read from here)
-    float* grad;             // flat FP32 gradient sums (training)
-    double* loss;            // sum of weighted squared errors / B (training)
+    float* gpart;            // training: per-CTA gradient sums [gridDim.x][P_TOTAL]
+    double* lpart;           // training: per-CTA loss sums [gridDim.x]
     float4* out;             // inference: network output (3 comps, scaled) per row
     int* err;
     int ntile, nrows;
@@ -287,35 +288,54 @@ __global__ void __launch_bounds__(128, 1) mlp_kernel(NetArgs A) {
         done++;
     }
 
-    if (TRAIN && !failed && done > 0) {
-        float* g = A.grad;
-        for (int c = 0; c < HID; c += 16) {
-            tm_ld16(trow + TM_DW2 + c, v);
+    if (TRAIN) {
+        // this CTA's gradient sums, plain stores into its own slice (reduced
+        // over CTAs by reduce_grad_kernel: no atomics, deterministic order)
+        float* g = A.gpart + (size_t)blockIdx.x * P_TOTAL;
+        float* red = reinterpret_cast<float*>(sm + SM_X);      // X tile no longer needed: 4 warps x 4 floats
+        if (!failed && done > 0) {
+            for (int c = 0; c < HID; c += 16) {
+                tm_ld16(trow + TM_DW2 + c, v);
 #pragma unroll
-            for (int j = 0; j < 16; j++) atomicAdd(g + P_W2 + tid * HID + c + j, v[j]);
+                for (int j = 0; j < 16; j++) g[P_W2 + tid * HID + c + j] = v[j];
+            }
+            for (int c = 0; c < K0; c += 16) {
+                tm_ld16(trow + TM_DW1 + c, v);
+#pragma unroll
+                for (int j = 0; j < 16; j++) g[P_W1 + tid * K0 + c + j] = v[j];
+            }
+            tm_ld16(trow + TM_DW3, v);
+#pragma unroll
+            for (int j = 0; j < NOP; j++) g[P_W3 + j * HID + tid] = v[j];
+            tm_ld16(trow + TM_DB1, v);
+            g[P_B1 + tid] = v[0];
+            tm_ld16(trow + TM_DB2, v);
+            g[P_B2 + tid] = v[0];
+        } else {
+            for (int i = tid; i < P_B3; i += 128) g[i] = 0.f;
         }
-        for (int c = 0; c < K0; c += 16) {
-            tm_ld16(trow + TM_DW1 + c, v);
-#pragma unroll
-            for (int j = 0; j < 16; j++) atomicAdd(g + P_W1 + tid * K0 + c + j, v[j]);
-        }
-        tm_ld16(trow + TM_DW3, v);
-#pragma unroll
-        for (int j = 0; j < NOP; j++) atomicAdd(g + P_W3 + j * HID + tid, v[j]);
-        tm_ld16(trow + TM_DB1, v);
-        atomicAdd(g + P_B1 + tid, v[0]);
-        tm_ld16(trow + TM_DB2, v);
-        atomicAdd(g + P_B2 + tid, v[0]);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
 #pragma unroll
             for (int k = 0; k < NOUT; k++) db3[k] += __shfl_xor_sync(0xffffffffu, db3[k], o);
         }
+        __syncthreads();
         if ((tid & 31) == 0) {
-            atomicAdd(A.loss, (double)lsum * (double)A.inv_batch);
+            red[4 * warp] = lsum;
 #pragma unroll
-            for (int k = 0; k < NOUT; k++) atomicAdd(g + P_B3 + k, db3[k]);
+            for (int k = 0; k < NOUT; k++) red[4 * warp + 1 + k] = db3[k];
+        }
+        __syncthreads();
+        if (tid < NOP) {
+            float b = 0.f;
+            if (tid < NOUT) for (int q = 0; q < 4; q++) b += red[4 * q + 1 + tid];
+            g[P_B3 + tid] = b;
+        }
+        if (tid == 0) {
+            double l = 0.0;
+            for (int q = 0; q < 4; q++) l += (double)red[4 * q];
+            A.lpart[blockIdx.x] = l * (double)A.inv_batch;
         }
     }
     if (failed && tid == 0) atomicExch(A.err, 1);
@@ -323,6 +343,22 @@ __global__ void __launch_bounds__(128, 1) mlp_kernel(NetArgs A) {
     __syncthreads();
     tc_after();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(TM_COLS) : "memory");
+}
+
+// sum of the per-CTA gradient slices (fixed order) and of the loss partials
+__global__ void reduce_grad_kernel(const float* __restrict__ gpart, const double* __restrict__ lpart, int nblk,
+                                   float* __restrict__ grad, double* __restrict__ loss) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < P_TOTAL) {
+        float acc = 0.f;
+        for (int b = 0; b < nblk; b++) acc += gpart[(size_t)b * P_TOTAL + i];
+        grad[i] = acc;
+    }
+    if (i == 0) {
+        double l = 0.0;
+        for (int b = 0; b < nblk; b++) l += lpart[b];
+        *loss = l;
+    }
 }
 
 // standardise raw features and pack them into bf16 core-matrix tiles
@@ -533,10 +569,10 @@ template <class X> struct Buf {
 struct Net {
     bool has_params = false;
     int t = 0;                              // AdamW step count
-    Buf<float> prm, grad, m, v, mean, istd, feat;
+    Buf<float> prm, grad, m, v, mean, istd, feat, gpart;
     Buf<uint8_t> Wp, Xs, Xd;
     Buf<float4> Td, outs, save;
-    Buf<double> loss, losses;
+    Buf<double> loss, losses, lpart;
     Buf<double4> E0;
     Buf<int> err, atom_sys, elem, accepted, keep;
     float out_scale = 1.f;
@@ -579,13 +615,18 @@ int pack_input(const float* d_feat, int n, int ntile, uint8_t* X, cudaStream_t s
 int run_net(bool train, const uint8_t* X, const float4* T, int ntile, int nrows, float inv_batch, float4* out,
             cudaStream_t st) {
     if (set_attr()) return -1;
+    const int grid = std::max(1, std::min(ntile, num_sms()));
+    if (train && (N.gpart.ensure((size_t)grid * P_TOTAL) || N.lpart.ensure(grid))) return -1;
     NetArgs a;
     a.X = reinterpret_cast<const uint4*>(X); a.T = T; a.Wp = reinterpret_cast<const uint4*>(N.Wp.p);
-    a.prm = N.prm.p; a.grad = N.grad.p; a.loss = N.loss.p; a.out = out; a.err = N.err.p;
+    a.prm = N.prm.p; a.gpart = N.gpart.p; a.lpart = N.lpart.p; a.out = out; a.err = N.err.p;
     a.ntile = ntile; a.nrows = nrows; a.inv_batch = inv_batch; a.out_scale = N.out_scale;
-    const int grid = std::max(1, std::min(ntile, num_sms()));
-    if (train) mlp_kernel<true><<<grid, 128, SM_ALLOC, st>>>(a);
-    else mlp_kernel<false><<<grid, 128, SM_ALLOC, st>>>(a);
+    if (train) {
+        mlp_kernel<true><<<grid, 128, SM_ALLOC, st>>>(a);
+        reduce_grad_kernel<<<(P_TOTAL + 255) / 256, 256, 0, st>>>(N.gpart.p, N.lpart.p, grid, N.grad.p, N.loss.p);
+    } else {
+        mlp_kernel<false><<<grid, 128, SM_ALLOC, st>>>(a);
+    }
     MCK(cudaGetLastError());
     return 0;
 }

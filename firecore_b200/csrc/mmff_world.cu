@@ -72,6 +72,13 @@ struct Bucket {
     std::vector<int> sys;          // system indices, largest first
     DBuf<int> queue;
     int smem = 0, grid = 0;
+    int cls = 0;                   // size class (see size_class)
+};
+
+// autotuned launch configuration of one size class (kind -1: heuristic)
+struct Tune {
+    int kind = -1, apl = 1, T = 0, S = 0;
+    float us_per_sys_step = 0.f;
 };
 
 struct World {
@@ -108,6 +115,14 @@ struct World {
     int force_T = 0, force_S = 0;
     std::vector<Bucket> buckets;
     bool buckets_dirty = true;
+    Tune tune[6];
+    // relax graph
+    bool use_graph = false, graph_valid = false;
+    cudaGraphExec_t gexec = nullptr;
+    int gkey_nstep = 0, gkey_mode = 0, gkey_version = -1;
+    bool gkey_count = false;
+    double gkey_fconv = 0.0;
+    int version = 0;               // bumped by every change of parameters or systems
 };
 
 World W;
@@ -166,63 +181,84 @@ Systems make_systems() {
 int pow2_floor(int x) { int p = 1; while (p * 2 <= x) p *= 2; return p; }
 
 // size buckets: thread count T >= atoms (<= 512); S lanes per atom in the pair sum
-int build_buckets() {
-    W.buckets.clear();
-    const int Ts[4] = {64, 128, 256, 512};
-    // groups 0/1: warp engine (<=32 / <=64 atoms), 2..5: CTA engine by thread count
-    std::vector<std::vector<int>> groups(6);
-    for (int s = 0; s < W.nsys; s++) {
-        const int na = W.natoms[s];
-        int b;
-        if (!W.force_T && na <= 32) b = 0;
-        else if (!W.force_T && na <= 64) b = 1;
-        else {
-            b = 5;
-            for (int k = 0; k < 4; k++) if (na <= Ts[k]) { b = 2 + k; break; }
-            if (W.force_T) { for (int k = 0; k < 4; k++) if (Ts[k] == W.force_T) b = 2 + k; }
-        }
-        groups[b].push_back(s);
-    }
-    int dev_smem = 0;
+// size class of a system: 0/1 warp engine (<=32 / <=64 atoms), 2..5 CTA
+// engine by thread count (<=64, <=128, <=256, larger)
+const int kClassT[4] = {64, 128, 256, 512};
+int size_class(int na) {
+    if (!W.force_T && na <= 32) return 0;
+    if (!W.force_T && na <= 64) return 1;
+    if (W.force_T) { for (int k = 0; k < 4; k++) if (kClassT[k] == W.force_T) return 2 + k; }
+    for (int k = 0; k < 4; k++) if (na <= kClassT[k]) return 2 + k;
+    return 5;
+}
+
+// launch configuration of a bucket whose systems are set: kind 1 = warp
+// engine (apl atoms per lane), kind 0 = CTA engine with T threads and S lanes
+// per atom in the pair sum.  Fills smem, grid; sets kernel attributes.
+int config_bucket(Bucket& B, int kind, int apl, int T, int S) {
+    int dev_smem = 0, nsm = 0;
     CK(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, W.device));
-    int nsm = 0;
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, W.device));
+    B.maxNA = 0; B.maxNN = 0;
+    for (int s : B.sys) { B.maxNA = std::max(B.maxNA, W.natoms[s]); B.maxNN = std::max(B.maxNN, W.nnode[s]); }
+    void* fns[2];
+    if (kind == 1) {
+        if (B.maxNA > 32 * apl) return fail("warp engine with %d atoms per lane cannot hold %d atoms", apl, B.maxNA);
+        B.kind = 1; B.apl = apl; B.T = 128; B.S = 1;
+        B.smem = 4 * warp_layout(B.maxNA, B.maxNN).per_warp;
+        fns[0] = relax_warp_fn(B.apl, false); fns[1] = relax_warp_fn(B.apl, true);
+    } else {
+        B.kind = 0; B.T = T; B.S = S;
+        B.smem = smem_layout(B.maxNA, B.maxNN, B.T).total;
+        fns[0] = relax_fn(B.T, B.S, false); fns[1] = relax_fn(B.T, B.S, true);
+    }
+    if (B.smem > dev_smem) return fail("system too large for shared memory: %d B > %d B", B.smem, dev_smem);
+    if (!fns[0] || !fns[1]) return fail("no kernel for bucket (kind %d, T=%d, S=%d)", B.kind, B.T, B.S);
+    for (int f = 0; f < 2; f++) CK(cudaFuncSetAttribute(fns[f], cudaFuncAttributeMaxDynamicSharedMemorySize, B.smem));
+    for (int e = 0; e < 2; e++) {
+        void* ef = B.kind ? eval_warp_fn(B.apl, e) : eval_fn(B.T, B.S, e);
+        CK(cudaFuncSetAttribute(ef, cudaFuncAttributeMaxDynamicSharedMemorySize, B.smem));
+    }
+    int occ = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fns[0], B.T, B.smem));
+    if (occ < 1) return fail("kernel cannot be resident (T=%d smem=%d)", B.T, B.smem);
+    const int per_block = B.kind ? 4 : 1;
+    const int nblk = ((int)B.sys.size() + per_block - 1) / per_block;
+    B.grid = std::min(nblk, occ * nsm);
+    if (B.queue.ensure(B.sys.size())) return -1;
+    CK(cudaMemcpy(B.queue.p, B.sys.data(), B.sys.size() * sizeof(int), cudaMemcpyHostToDevice));
+    return 0;
+}
+
+// heuristic configuration of a size class: warp engine for <= 64 atoms, else
+// the class's thread count with pair lanes filling the block
+void default_config(int cls, int maxNA, int& kind, int& apl, int& T, int& S) {
+    if (cls <= 1) { kind = 1; apl = cls + 1; T = 128; S = 1; return; }
+    kind = 0; apl = 1; T = kClassT[cls - 2];
+    S = std::min(pow2_floor(std::max(1, T / std::max(1, maxNA))), 8);
+    if (W.force_S) S = W.force_S;
+}
+
+int build_buckets() {
+    for (auto& B : W.buckets) B.queue.release();
+    W.buckets.clear();
+    W.graph_valid = false;
+    std::vector<std::vector<int>> groups(6);
+    for (int s = 0; s < W.nsys; s++) groups[size_class(W.natoms[s])].push_back(s);
     // largest systems first: their buckets are launched first
     for (int k = 5; k >= 0; k--) {
         if (groups[k].empty()) continue;
         Bucket B;
         B.sys = groups[k];
         std::stable_sort(B.sys.begin(), B.sys.end(), [](int a, int b) { return W.natoms[a] > W.natoms[b]; });
-        for (int s : B.sys) { B.maxNA = std::max(B.maxNA, W.natoms[s]); B.maxNN = std::max(B.maxNN, W.nnode[s]); }
-        void* fns[3];
-        if (k <= 1) {
-            B.kind = 1; B.apl = k + 1; B.T = 128; B.S = 1;
-            B.smem = 4 * warp_layout(B.maxNA, B.maxNN).per_warp;
-            fns[0] = relax_warp_fn(B.apl, false); fns[1] = relax_warp_fn(B.apl, true);
-            fns[2] = nullptr;
-        } else {
-            B.kind = 0; B.T = Ts[k - 2];
-            int S = pow2_floor(std::max(1, B.T / std::max(1, B.maxNA)));
-            B.S = std::min(S, 8);
-            if (W.force_S) B.S = W.force_S;
-            B.smem = smem_layout(B.maxNA, B.maxNN, B.T).total;
-            fns[0] = relax_fn(B.T, B.S, false); fns[1] = relax_fn(B.T, B.S, true); fns[2] = nullptr;
-        }
-        if (B.smem > dev_smem) return fail("system too large for shared memory: %d B > %d B", B.smem, dev_smem);
-        if (!fns[0] || !fns[1]) return fail("no kernel for bucket (kind %d, T=%d, S=%d)", B.kind, B.T, B.S);
-        for (int f = 0; f < 2; f++) CK(cudaFuncSetAttribute(fns[f], cudaFuncAttributeMaxDynamicSharedMemorySize, B.smem));
-        for (int e = 0; e < 2; e++) {
-            void* ef = B.kind ? eval_warp_fn(B.apl, e) : eval_fn(B.T, B.S, e);
-            CK(cudaFuncSetAttribute(ef, cudaFuncAttributeMaxDynamicSharedMemorySize, B.smem));
-        }
-        int occ = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fns[0], B.T, B.smem));
-        if (occ < 1) return fail("kernel cannot be resident (T=%d smem=%d)", B.T, B.smem);
-        const int per_block = B.kind ? 4 : 1;
-        const int nblk = ((int)B.sys.size() + per_block - 1) / per_block;
-        B.grid = std::min(nblk, occ * nsm);
-        if (B.queue.ensure(B.sys.size())) return -1;
-        CK(cudaMemcpy(B.queue.p, B.sys.data(), B.sys.size() * sizeof(int), cudaMemcpyHostToDevice));
+        int maxNA = 0;
+        for (int s : B.sys) maxNA = std::max(maxNA, W.natoms[s]);
+        int kind, apl, T, S;
+        default_config(k, maxNA, kind, apl, T, S);
+        const Tune& tu = W.tune[k];
+        if (tu.kind >= 0 && !W.force_T && !W.force_S) { kind = tu.kind; apl = tu.apl; T = tu.T; S = tu.S; }
+        if (config_bucket(B, kind, apl, T, S)) return -1;
+        B.cls = k;
         W.buckets.push_back(std::move(B));
     }
     while (W.bstreams.size() < W.buckets.size()) {
@@ -236,6 +272,34 @@ int build_buckets() {
 template <class X> int upload(DBuf<X>& d, const std::vector<X>& h) {
     if (d.ensure(h.size())) return -1;
     if (!h.empty()) CK(cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(X), cudaMemcpyHostToDevice, W.stream));
+    return 0;
+}
+
+// the launches of one relax call on the library stream: reset the work
+// counters, fork to one stream per bucket, one persistent kernel per bucket
+// (systems claimed through the bucket's queue), join
+int enqueue_relax(const Params& P) {
+    Params Pc = P;
+    Systems Y = make_systems();
+    CK(cudaMemsetAsync(W.d_counter.p, 0, 64 * sizeof(int), W.stream));
+    CK(cudaEventRecord(W.evfork, W.stream));
+    for (size_t b = 0; b < W.buckets.size(); b++) {
+        Bucket& B = W.buckets[b];
+        cudaStream_t st = W.bstreams[b];
+        CK(cudaStreamWaitEvent(st, W.evfork, 0));
+        void* fn = B.kind ? relax_warp_fn(B.apl, W.count) : relax_fn(B.T, B.S, W.count);
+        const int* q = B.queue.p;
+        int nq = (int)B.sys.size();
+        int* ctr = W.d_counter.p + b;
+        int mna = B.maxNA, mnn = B.maxNN;
+        void* args[] = {&Pc, &Y, &q, &nq, &ctr, &mna, &mnn};
+        CK(cudaLaunchKernel(fn, dim3(B.grid), dim3(B.T), args, B.smem, st));
+    }
+    for (size_t b = 0; b < W.buckets.size(); b++) {
+        CK(cudaEventRecord(W.bev[b], W.bstreams[b]));
+        CK(cudaStreamWaitEvent(W.stream, W.bev[b], 0));
+    }
+    CK(cudaGetLastError());
     return 0;
 }
 
@@ -281,6 +345,7 @@ int mmff_sync(void) {
 }
 
 int mmff_set_params(int flags, const int* nPBC, double Rcut, double alphaMorse, double FmaxNonBonded) {
+    W.version++;
     W.flags = flags;
     if (nPBC) for (int k = 0; k < 3; k++) W.npbc[k] = nPBC[k];
     W.Rcut = Rcut;
@@ -291,6 +356,7 @@ int mmff_set_params(int flags, const int* nPBC, double Rcut, double alphaMorse, 
 
 int mmff_set_fire(double dt_max, double dt_min, double damp_max, double finc, double fdec, double falpha,
                   int minLastNeg, double cv_kill, double Flim, int variant) {
+    W.version++;
     if (variant != 0 && variant != 1) return fail("FIRE variant must be 0 or 1");
     double f[10] = {dt_max, dt_min, damp_max, finc, fdec, falpha, (double)minLastNeg, cv_kill, Flim, (double)variant};
     memcpy(W.fire, f, sizeof f);
@@ -305,6 +371,7 @@ int mmff_set_launch(int threads, int pair_split) {
 }
 
 int mmff_grid_upload(int nx, int ny, int nz, const double* pos0, const double* step, const double* coefs) {
+    W.version++;
     if (ensure_ready()) return -1;
     if (nx < 4 || ny < 4 || nz < 8) return fail("grid too small (%d,%d,%d)", nx, ny, nz);
     const size_t n = (size_t)nx * ny * nz;
@@ -321,6 +388,7 @@ int mmff_grid_upload(int nx, int ny, int nz, const double* pos0, const double* s
 int mmff_grid_build(int nsub, const double* spos, const double* sREQ, const double* lvec, const int* nPBC_mors,
                     const int* nPBC_coul, double alphaMorse, int nx, int ny, int nz, const double* pos0,
                     const double* step, double* coefs_out) {
+    W.version++;
     if (ensure_ready()) return -1;
     if (nx < 4 || ny < 4 || nz < 8 || nsub < 1) return fail("bad grid build arguments");
     const long ntot = (long)nx * ny * nz;
@@ -513,27 +581,147 @@ int mmff_relax(int nstep_max, double Fconv, int conv_mode) {
     if (!W.nsys) return fail("no systems uploaded");
     if (W.buckets_dirty && build_buckets()) return -1;
     Params P = make_params(false, nstep_max, Fconv, conv_mode);
+    if (!W.use_graph) return enqueue_relax(P);
+    // one CUDA graph per (parameters, step limit, criterion): the counter reset,
+    // the fork to the bucket streams, every bucket's persistent kernel and the join
+    const bool same = W.graph_valid && W.gkey_nstep == nstep_max && W.gkey_fconv == Fconv &&
+                      W.gkey_mode == conv_mode && W.gkey_count == W.count && W.gkey_version == W.version;
+    if (!same) {
+        if (W.gexec) { cudaGraphExecDestroy(W.gexec); W.gexec = nullptr; }
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(W.stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = enqueue_relax(P);
+        const cudaError_t e = cudaStreamEndCapture(W.stream, &g);
+        if (rc) { if (g) cudaGraphDestroy(g); return -1; }
+        if (e != cudaSuccess) return fail("relax graph capture: %s", cudaGetErrorString(e));
+        const cudaError_t ei = cudaGraphInstantiate(&W.gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) { W.gexec = nullptr; return fail("relax graph instantiate: %s", cudaGetErrorString(ei)); }
+        W.graph_valid = true; W.gkey_nstep = nstep_max; W.gkey_fconv = Fconv; W.gkey_mode = conv_mode;
+        W.gkey_count = W.count; W.gkey_version = W.version;
+    }
+    CK(cudaGraphLaunch(W.gexec, W.stream));
+    return 0;
+}
+
+// Relax through a captured CUDA graph (on != 0) or direct launches.
+int mmff_set_graph(int on) {
+    W.use_graph = on != 0;
+    return 0;
+}
+
+// ---------------------------------------------------------------- autotuner
+namespace {
+struct Cand { int kind, apl, T, S; };
+std::vector<Cand> candidates(int cls) {
+    switch (cls) {
+        case 0: return {{1, 1, 128, 1}, {0, 1, 64, 1}, {0, 1, 64, 2}, {0, 1, 64, 4}, {0, 1, 128, 2}, {0, 1, 128, 4}};
+        case 1: return {{1, 2, 128, 1}, {0, 1, 64, 1}, {0, 1, 64, 2}, {0, 1, 128, 1}, {0, 1, 128, 2}, {0, 1, 128, 4}};
+        case 3: return {{0, 1, 64, 1}, {0, 1, 64, 2}, {0, 1, 128, 1}, {0, 1, 128, 2}, {0, 1, 128, 4}, {0, 1, 256, 2}, {0, 1, 256, 4}};
+        case 4: return {{0, 1, 128, 1}, {0, 1, 128, 2}, {0, 1, 256, 1}, {0, 1, 256, 2}, {0, 1, 512, 1}, {0, 1, 512, 2}};
+        case 5: return {{0, 1, 256, 1}, {0, 1, 256, 2}, {0, 1, 512, 1}, {0, 1, 512, 2}, {0, 1, 512, 4}};
+        default: return {};
+    }
+}
+}  // namespace
+
+// Time every candidate launch configuration of each size class present on a
+// sample of that class's systems (nstep_probe FIRE steps, no convergence
+// exit) and keep the fastest for later relax/eval calls.  Positions,
+// velocities and FIRE state are restored afterwards.  report (nullable):
+// 6 floats per candidate tried (class, kind, atoms per lane, threads, pair
+// lanes, microseconds per system-step; negative: not launchable).
+int mmff_autotune(int nstep_probe, int max_sample, float* report, int report_cap) {
+    if (ensure_ready()) return -1;
+    if (!W.nsys) return fail("no systems uploaded");
+    if (nstep_probe < 1 || max_sample < 1) return fail("autotune: nstep_probe and max_sample must be >= 1");
+    if (W.force_T || W.force_S) return fail("autotune: clear mmff_set_launch overrides first");
+    DBuf<float4> sp, sv; DBuf<double4> sf; DBuf<int> sst, sns; DBuf<float> sfc;
+    if (sp.ensure(W.NV) || sv.ensure(W.NV) || sf.ensure(W.nsys) || sst.ensure(W.nsys) || sns.ensure(W.nsys) ||
+        sfc.ensure(W.nsys))
+        return -1;
+    auto copy_state = [&](bool save) -> int {
+        auto cp = [&](void* a, void* b, size_t n) { return cudaMemcpyAsync(save ? a : b, save ? b : a, n, cudaMemcpyDeviceToDevice, W.stream); };
+        CK(cp(sp.p, W.d_pos.p, W.NV * sizeof(float4)));
+        CK(cp(sv.p, W.d_vel.p, W.NV * sizeof(float4)));
+        CK(cp(sf.p, W.d_fire.p, W.nsys * sizeof(double4)));
+        CK(cp(sst.p, W.d_status.p, W.nsys * sizeof(int)));
+        CK(cp(sns.p, W.d_nsteps.p, W.nsys * sizeof(int)));
+        CK(cp(sfc.p, W.d_fconv.p, W.nsys * sizeof(float)));
+        return 0;
+    };
+    if (copy_state(true)) return -1;
+    std::vector<std::vector<int>> groups(6);
+    for (int s = 0; s < W.nsys; s++) groups[size_class(W.natoms[s])].push_back(s);
+    Params P = make_params(false, nstep_probe, 0.0, 1);     // Fmax < 0: never converges
     Systems Y = make_systems();
-    CK(cudaMemsetAsync(W.d_counter.p, 0, 64 * sizeof(int), W.stream));
-    CK(cudaEventRecord(W.evfork, W.stream));
-    for (size_t b = 0; b < W.buckets.size(); b++) {
-        Bucket& B = W.buckets[b];
-        cudaStream_t st = W.bstreams[b];
-        CK(cudaStreamWaitEvent(st, W.evfork, 0));
-        void* fn = B.kind ? relax_warp_fn(B.apl, W.count) : relax_fn(B.T, B.S, W.count);
-        const int* q = B.queue.p;
-        int nq = (int)B.sys.size();
-        int* ctr = W.d_counter.p + b;
-        int mna = B.maxNA, mnn = B.maxNN;
-        void* args[] = {&P, &Y, &q, &nq, &ctr, &mna, &mnn};
-        CK(cudaLaunchKernel(fn, dim3(B.grid), dim3(B.T), args, B.smem, st));
+    int nrep = 0;
+    for (int cls = 0; cls < 6; cls++) {
+        std::vector<int>& g = groups[cls];
+        if (g.empty()) continue;
+        std::stable_sort(g.begin(), g.end(), [](int a, int b) { return W.natoms[a] > W.natoms[b]; });
+        std::vector<int> sample;
+        const int ns = std::min<int>(max_sample, (int)g.size());
+        for (int i = 0; i < ns; i++) sample.push_back(g[(size_t)i * g.size() / ns]);
+        float best = 1e30f;
+        Tune bt;
+        for (const Cand& c : candidates(cls)) {
+            Bucket B;
+            B.sys = sample;
+            float us = -1.f;
+            if (config_bucket(B, c.kind, c.apl, c.T, c.S) == 0) {
+                void* fn = B.kind ? relax_warp_fn(B.apl, false) : relax_fn(B.T, B.S, false);
+                const int* q = B.queue.p;
+                int nq = (int)B.sys.size(), mna = B.maxNA, mnn = B.maxNN;
+                int* ctr = W.d_counter.p + 32;
+                void* args[] = {&P, &Y, &q, &nq, &ctr, &mna, &mnn};
+                float ms = 0.f;
+                for (int rep = 0; rep < 2; rep++) {        // first launch warms caches and clocks
+                    if (copy_state(false)) return -1;
+                    CK(cudaMemsetAsync(ctr, 0, sizeof(int), W.stream));
+                    CK(cudaEventRecord(W.ev0, W.stream));
+                    CK(cudaLaunchKernel(fn, dim3(B.grid), dim3(B.T), args, B.smem, W.stream));
+                    CK(cudaEventRecord(W.ev1, W.stream));
+                    CK(cudaEventSynchronize(W.ev1));
+                    CK(cudaEventElapsedTime(&ms, W.ev0, W.ev1));
+                }
+                us = 1e3f * ms / ((float)ns * (float)nstep_probe);
+                if (us < best) { best = us; bt.kind = c.kind; bt.apl = c.apl; bt.T = c.T; bt.S = c.S; bt.us_per_sys_step = us; }
+            } else {
+                cudaGetLastError();
+            }
+            B.queue.release();
+            if (report && nrep < report_cap) {
+                const float row[6] = {(float)cls, (float)c.kind, (float)c.apl, (float)c.T, (float)c.S, us};
+                for (int j = 0; j < 6; j++) report[6 * nrep + j] = row[j];
+            }
+            nrep++;
+        }
+        if (bt.kind >= 0) W.tune[cls] = bt;
     }
-    // join the bucket streams back into the library stream
-    for (size_t b = 0; b < W.buckets.size(); b++) {
-        CK(cudaEventRecord(W.bev[b], W.bstreams[b]));
-        CK(cudaStreamWaitEvent(W.stream, W.bev[b], 0));
-    }
-    CK(cudaGetLastError());
+    if (copy_state(false)) return -1;
+    CK(cudaStreamSynchronize(W.stream));
+    W.buckets_dirty = true;
+    g_err.clear();
+    return nrep;
+}
+
+// Tuned configuration of a size class: out = (kind, atoms per lane, threads,
+// pair lanes); kind -1 = heuristic.  Set it back (e.g. from a saved file).
+int mmff_get_tuning(int cls, int* out) {
+    if (cls < 0 || cls > 5) return fail("size class must be 0..5");
+    const Tune& t = W.tune[cls];
+    out[0] = t.kind; out[1] = t.apl; out[2] = t.T; out[3] = t.S;
+    return 0;
+}
+
+int mmff_set_tuning(int cls, int kind, int apl, int T, int S) {
+    if (cls < 0 || cls > 5) return fail("size class must be 0..5");
+    if (kind == 1 && !((cls == 0 && apl == 1) || (cls == 1 && apl == 2))) return fail("warp engine only for classes 0/1 (apl = class + 1)");
+    if (kind == 0 && !relax_fn(T, S, false)) return fail("no CTA kernel with T=%d S=%d", T, S);
+    if (kind != -1 && kind != 0 && kind != 1) return fail("kind must be -1, 0 or 1");
+    W.tune[cls].kind = kind; W.tune[cls].apl = apl; W.tune[cls].T = T; W.tune[cls].S = S;
+    W.buckets_dirty = true;
     return 0;
 }
 

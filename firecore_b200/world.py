@@ -7,6 +7,8 @@ raises ``RuntimeError`` if the library or a CUDA device is missing.
 from __future__ import annotations
 
 import ctypes
+import json
+import os
 from dataclasses import dataclass
 
 import numpy as np
@@ -67,6 +69,48 @@ class World:
 
     def set_launch(self, threads=0, pair_split=0):
         _check(self.lib.mmff_set_launch(threads, pair_split), "mmff_set_launch")
+
+    def set_graph(self, on: bool = True):
+        """Replay mmff_relax as one captured CUDA graph per parameter set."""
+        _check(self.lib.mmff_set_graph(int(on)), "mmff_set_graph")
+
+    # ---------------------------------------------------------------- autotuner
+    SIZE_CLASSES = {0: "<=32 atoms", 1: "<=64 atoms", 2: "<=64 atoms (forced CTA)", 3: "<=128 atoms",
+                    4: "<=256 atoms", 5: ">256 atoms"}
+
+    def autotune(self, nstep_probe: int = 50, max_sample: int = 256, path: str | None = None):
+        """Time the candidate launch configurations of every size class present
+        and keep the fastest; with ``path``, the choice is saved as JSON."""
+        rep = np.zeros((64, 6), np.float32)
+        n = _check(self.lib.mmff_autotune(int(nstep_probe), int(max_sample), _lib.ptr(rep), 64), "mmff_autotune")
+        rows = [dict(size_class=int(r[0]), kind="warp" if r[1] == 1 else "cta", atoms_per_lane=int(r[2]),
+                     threads=int(r[3]), pair_lanes=int(r[4]), us_per_system_step=float(r[5])) for r in rep[:min(n, 64)]]
+        if path:
+            self.save_tuning(path, rows)
+        return rows
+
+    def tuning(self):
+        out = {}
+        for c in range(6):
+            t = np.zeros(4, np.int32)
+            _check(self.lib.mmff_get_tuning(c, _lib.ptr(t)), "mmff_get_tuning")
+            if t[0] >= 0:
+                out[c] = dict(kind=int(t[0]), atoms_per_lane=int(t[1]), threads=int(t[2]), pair_lanes=int(t[3]))
+        return out
+
+    def save_tuning(self, path: str, report=None):
+        doc = {"tuning": {str(c): v for c, v in self.tuning().items()}, "report": report or []}
+        with open(path, "w") as f:
+            json.dump(doc, f, indent=1)
+
+    def load_tuning(self, path: str) -> bool:
+        if not os.path.exists(path):
+            return False
+        doc = json.load(open(path))
+        for c, v in doc.get("tuning", {}).items():
+            _check(self.lib.mmff_set_tuning(int(c), v["kind"], v["atoms_per_lane"], v["threads"], v["pair_lanes"]),
+                   "mmff_set_tuning")
+        return True
 
     def grid_upload(self, coefs: np.ndarray, grid: GridSpec):
         c = np.ascontiguousarray(coefs, np.float64)

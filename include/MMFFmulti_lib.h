@@ -117,6 +117,25 @@ int mmff_eval(int with_energy);
  * (MolWorld_sp3_multi.h:1694-1846) with per-system FIRE in FP64 on the device
  * and no host round trip.  Asynchronous: mmff_sync / mmff_get_* wait. */
 int mmff_relax(int nstep_max, double Fconv, int conv_mode);
+/* on != 0: mmff_relax replays one captured CUDA graph (counter reset, fork
+ * to the per-bucket streams, every bucket's persistent kernel, join) per
+ * (parameters, nstep_max, Fconv, conv_mode); off (default): direct launches.
+ * Replaces the reference's host loop of kernel enqueues and round trips
+ * every 10 steps (MolWorld_sp3_multi.h:843-908). */
+int mmff_set_graph(int on);
+/* Autotuner (no counterpart in the reference, which uses one fixed work-group
+ * size): for each size class present (0: <= 32 atoms, 1: <= 64, 3: <= 128,
+ * 4: <= 256, 5: larger), time every candidate launch configuration (warp per
+ * system, or threads per CTA x lanes per atom in the pair sum) on up to
+ * max_sample of its systems for nstep_probe FIRE steps and keep the fastest.
+ * State is restored.  report [6 per candidate] (nullable): class, kind,
+ * atoms per lane, threads, pair lanes, us per system-step (< 0: not
+ * launchable).  Returns the number of candidates tried. */
+int mmff_autotune(int nstep_probe, int max_sample, float* report, int report_cap);
+/* Tuned configuration of size class cls: out[4] = (kind: -1 heuristic, 0 CTA
+ * per system, 1 warp per system; atoms per lane; threads; pair lanes). */
+int mmff_get_tuning(int cls, int* out);
+int mmff_set_tuning(int cls, int kind, int apl, int threads, int pair_split);
 
 /* ------------------------------------------------------------ results */
 int mmff_get_forces(double* force);                 /* [sum nvecs][3] */

@@ -1,0 +1,84 @@
+"""Uneven batching on the GPU: the captured relax graph, the launch-
+configuration autotuner and its JSON persistence, and retire/refill of the
+per-bucket work queues over mixed system sizes."""
+import numpy as np
+import pytest
+
+from conftest import grid_from_golden
+from firecore_b200 import systems as S
+from firecore_b200.world import DEFAULT_FLAGS, FireParams, World
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def world():
+    return World(0)
+
+
+def uneven(world, golden, n=96, seed=5, lo=20, hi=300):
+    grid = grid_from_golden(golden)
+    sizes = S.loguniform_sizes(n, seed, lo, hi)
+    b = S.make_systems(sizes, seed, topo_mode=1, sigma=0.1, rotate=True, cell=(22.56, 22.56, 40.0))
+    world.set_params(flags=DEFAULT_FLAGS, Rcut=10.0)
+    world.set_fire(FireParams(Flim=10.0))
+    world.grid_upload(golden["C"], grid)
+    world.upload(b)
+    return b
+
+
+def test_graph_relax_is_identical_to_direct_launches(world, golden):
+    b = uneven(world, golden)
+    world.set_graph(False)
+    world.restore(); world.relax(300, 1e-4, conv_mode=1)
+    d = world.state()
+    world.set_graph(True)
+    for _ in range(2):                       # capture, then replay of the cached graph
+        world.restore(); world.relax(300, 1e-4, conv_mode=1)
+        g = world.state()
+        assert np.array_equal(d["pos"], g["pos"]) and np.array_equal(d["status"], g["status"])
+        assert np.array_equal(d["nsteps"], g["nsteps"])
+    world.restore(); world.relax(100, 1e-4, conv_mode=1)         # new key: recaptured
+    assert (world.state()["nsteps"] <= 100).all()
+    world.set_graph(False)
+
+
+def test_autotune_picks_a_launchable_config_and_keeps_physics(world, golden, tmp_path):
+    b = uneven(world, golden)
+    for c in range(6):
+        world.lib.mmff_set_tuning(c, -1, 1, 0, 0)
+    world.restore(); world.relax(200, 1e-4, conv_mode=1)
+    _, E_def = world.eval()
+    rows = world.autotune(nstep_probe=20, max_sample=32, path=str(tmp_path / "tune.json"))
+    assert rows and all(r["us_per_system_step"] > 0 or r["us_per_system_step"] < 0 for r in rows)
+    tuned = world.tuning()
+    classes = {r["size_class"] for r in rows}
+    assert set(tuned) == classes
+    for c, t in tuned.items():
+        ok = [r for r in rows if r["size_class"] == c and r["us_per_system_step"] > 0]
+        best = min(ok, key=lambda r: r["us_per_system_step"])
+        assert (t["threads"], t["pair_lanes"]) == (best["threads"], best["pair_lanes"])
+    world.restore(); world.relax(200, 1e-4, conv_mode=1)
+    _, E_tun = world.eval()
+    # launch shape changes only the summation order of the pair sums
+    assert np.allclose(E_tun[:, 3], E_def[:, 3], rtol=1e-4, atol=1e-4)
+    # persistence round trip
+    for c in range(6):
+        world.lib.mmff_set_tuning(c, -1, 1, 0, 0)
+    assert world.tuning() == {}
+    assert world.load_tuning(str(tmp_path / "tune.json"))
+    assert world.tuning() == tuned
+
+
+def test_queue_retires_and_refills_mixed_sizes(world, golden):
+    """Many more systems than resident slots, sizes 20..400: every system is
+    claimed exactly once per call (nsteps set for all) and converged systems
+    carry their converging step."""
+    b = uneven(world, golden, n=3000, seed=9, lo=20, hi=400)
+    world.set_graph(True)
+    world.restore(); world.relax(400, 1e-4, conv_mode=1)
+    st = world.state()
+    assert ((st["status"] == 1) | (st["status"] == 2) | (st["status"] == -1)).all()
+    assert (st["nsteps"] > 0).all() and (st["nsteps"] <= 400).all()
+    assert (st["nsteps"][st["status"] == 2] == 400).all()
+    world.set_graph(False)

@@ -64,7 +64,10 @@ def test_forward_vs_oracle(world):
     prop.set_params(p, mean, std, s)
     y = prop.infer(F)
     yo = M.forward(Xo, p, bf=True)[0][:, :3] * s
-    assert np.abs(y - yo).max() <= 1e-3 * np.abs(yo).max(), np.abs(y - yo).max()
+    # FP32 vs FP64 pre-activations can round a hidden activation to the
+    # neighbouring bf16 value (2^-8 relative): rare outliers, bounded
+    err = np.abs(y - yo) / np.abs(yo).max()
+    assert np.quantile(err, 0.99) <= 1e-5 and err.max() <= 5e-3, (np.quantile(err, 0.99), err.max())
 
 
 def test_adamw_vs_oracle(world):
