@@ -153,6 +153,11 @@ def run_ours(args):
     w.upload(batch)
     nsys = batch.nsys
     natoms = batch.natoms.astype(np.int64)
+    # launch shapes from the autotuner (untimed; the choice is reported)
+    t0 = time.perf_counter()
+    tune_rows = w.autotune(nstep_probe=50, max_sample=512) if not args.no_tune else []
+    tune_s = time.perf_counter() - t0
+    w.set_graph(True)
     # counting pass (untimed): algorithmic work of one relaxation of this batch
     lib.mmff_set_counting(1)
     w.restore(); w.relax(MAXSTEPS, FCONV, 1)
@@ -209,17 +214,9 @@ def run_ours(args):
         h2d = nv * 16 * 2 + nsys * 32
         d2h = nv * 16 * 2 + nsys * (32 + 4 + 4 + 4)
         e2e = {"value": conv_e2e / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
-    # aggregate over ranks: converged systems summed, time = max over ranks
-    tot_conv, t_max = conv, t_dev
-    if dist:
-        tt = torch.tensor([float(conv), t_dev], device="cuda", dtype=torch.float64)
-        c_t = tt[0:1].clone(); dist.all_reduce(c_t)
-        m_t = tt[1:2].clone(); dist.all_reduce(m_t, op=dist.ReduceOp.MAX)
-        tot_conv, t_max = float(c_t.item()), float(m_t.item())
-        if e2e:
-            ee = torch.tensor([e2e["value"]], device="cuda", dtype=torch.float64)
-            dist.all_reduce(ee)
-            e2e["value"] = float(ee.item())
+    tot_conv, t_max, e2e_v = aggregate_ranks(conv, t_dev, e2e["value"] if e2e else None, dist, "cuda")
+    if e2e:
+        e2e["value"] = e2e_v
     value = tot_conv / t_max
     ms_step = 1e3 * t_max / args.steps
     # roofline of the relax kernel: pair term on FP32 CUDA cores
@@ -267,13 +264,30 @@ def run_ours(args):
                                        "method": "200-step relax with all terms minus without GridFF"},
                          "term_times_ms": attr_t},
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
-            "buckets": w.buckets(),
+            "buckets": w.buckets(), "relax_graph": True,
+            "autotune": {"seconds": tune_s, "chosen": {str(k): v for k, v in w.tuning().items()},
+                         "candidates": [[r["size_class"], r["kind"], r["threads"], r["pair_lanes"],
+                                         round(r["us_per_system_step"], 4)] for r in tune_rows]},
         }
         print(json.dumps(out))
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     return out
+
+
+def aggregate_ranks(conv, t_dev, e2e_value, dist, device):
+    """Whole-job numbers of the replica ranks (disjoint systems, no exchange on
+    the data path): converged systems and end-to-end rates summed, device time
+    the maximum over ranks.  Every rank makes the same two collective calls."""
+    if dist is None:
+        return float(conv), float(t_dev), e2e_value
+    import torch
+    s = torch.tensor([float(conv), 0.0 if e2e_value is None else float(e2e_value)], device=device, dtype=torch.float64)
+    dist.all_reduce(s)
+    m = torch.tensor([float(t_dev)], device=device, dtype=torch.float64)
+    dist.all_reduce(m, op=dist.ReduceOp.MAX)
+    return float(s[0]), float(m[0]), (None if e2e_value is None else float(s[1]))
 
 
 def term_attribution(w, lib, nsteps=200):
@@ -528,6 +542,7 @@ def main():
     ap.add_argument("--train-steps", type=int, default=2000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner (heuristic shapes)")
     ap.add_argument("--maxsteps", type=int, default=MAXSTEPS, help="FIRE step limit per system (profiling runs use fewer)")
     args = ap.parse_args()
     MAXSTEPS = args.maxsteps

@@ -343,14 +343,23 @@ __device__ __forceinline__ float4 grid_atom(const Params& P, float3 u, float4 PL
 
 // ---- shared-memory carve-up of one system (byte offsets)
 struct SmemLayout {
-    int maxNA, maxNN, maxNV, nwarps;
+    int maxNA, maxNN, maxNV, nwarps, nimg, nwords;
     // offsets in bytes
-    int pos, vel, fasm, fnb, fgrid, REQ, PLQ, ng, ngC, bk, apar, bL, bK, ksp, kpp, fng, red, total;
+    int pos, vel, fasm, fnb, fgrid, REQ, PLQ, ng, ngC, bk, apar, bL, bK, ksp, kpp, fng, red;
+    int cwords, cpref, ccnt, clist, total;     // per-image candidate lists (cutoff + PBC only)
 };
 
-__host__ __device__ inline SmemLayout smem_layout(int maxNA, int maxNN, int T) {
+// number of shifted (non-central) PBC images of the pair term
+__host__ __device__ inline int shifted_images(int flags, const int* npbc) {
+    if (!(flags & F_PBC)) return 0;
+    return (2 * npbc[0] + 1) * (2 * npbc[1] + 1) * (2 * npbc[2] + 1) - 1;
+}
+
+// nimg: shifted images that get candidate lists (0: none)
+__host__ __device__ inline SmemLayout smem_layout(int maxNA, int maxNN, int T, int nimg) {
     SmemLayout L;
     L.maxNA = maxNA; L.maxNN = maxNN; L.maxNV = maxNA + maxNN; L.nwarps = T / 32;
+    L.nimg = nimg; L.nwords = (maxNA + 31) / 32;
     int o = 0;
     auto take = [&](int bytes) { int r = o; o += (bytes + 15) & ~15; return r; };
     L.pos = take(16 * L.maxNV);
@@ -370,6 +379,10 @@ __host__ __device__ inline SmemLayout smem_layout(int maxNA, int maxNN, int T) {
     L.kpp = take(16 * maxNN);
     L.fng = take(16 * 8 * maxNN);
     L.red = take(128 * L.nwarps + 64);     // per warp: 4 doubles (32 B) at 0, bbox 6 floats at 64*nwarps
+    L.cwords = take(4 * nimg * L.nwords);   // candidate bit words per image
+    L.cpref = take(4 * nimg * L.nwords);    // exclusive prefix of their popcounts
+    L.ccnt = take(4 * nimg);                // candidates per image
+    L.clist = take(2 * nimg * maxNA);       // candidate atom indices per image, ascending
     L.total = o;
     return L;
 }

@@ -59,6 +59,7 @@ struct Engine {
     float3 gorg;
     // per-step image culling
     float bbmin[3], bbmax[3];
+    bool hasH = false;          // any H-bond pseudo-charge in the system (block-uniform)
     // pair-images evaluated by this thread (COUNT builds only)
     unsigned long long npair = 0;
 
@@ -82,10 +83,13 @@ struct Engine {
         for (int v = tid; v < nvecs; v += T) { spos[v] = Y.pos[voff + v]; svel[v] = Y.vel[voff + v]; }
         float4* sREQ = at<float4>(L.REQ); float4* sPLQ = at<float4>(L.PLQ);
         int4* sng = at<int4>(L.ng); int4* sngC = at<int4>(L.ngC); int4* sbk = at<int4>(L.bk);
+        int h = 0;
         for (int a = tid; a < natoms; a += T) {
-            sREQ[a] = Y.REQ[aoff + a]; sPLQ[a] = Y.PLQ[aoff + a];
+            const float4 r = Y.REQ[aoff + a];
+            sREQ[a] = r; sPLQ[a] = Y.PLQ[aoff + a]; h |= (r.w != 0.f);
             sng[a] = Y.neighs[aoff + a]; sngC[a] = Y.neighCell[aoff + a]; sbk[a] = Y.bkneighs[aoff + a];
         }
+        hasH = __syncthreads_or(h) != 0;
         float4* sap = at<float4>(L.apar); float4* sbL = at<float4>(L.bL); float4* sbK = at<float4>(L.bK);
         float4* sks = at<float4>(L.ksp); float4* skp = at<float4>(L.kpp);
         for (int n = tid; n < nnode; n += T) {
@@ -136,6 +140,116 @@ struct Engine {
         return gx * gx + gy * gy + gz * gz < P.Rc2;
     }
 
+    // Candidate lists of the shifted images: atom j is a candidate of image
+    // (ix,iy,iz) when its shifted position lies within the cutoff of this
+    // system's own bounding box (no atom i can reach the others).  Lists are
+    // ascending in j (ballot words, per-image prefix sums), so the pair sums
+    // keep a fixed order.  All threads; contains barriers.
+    __device__ void build_candidates() {
+        const float4* spos = at<float4>(L.pos);
+        uint32_t* words = at<uint32_t>(L.cwords);
+        int* pref = at<int>(L.cpref);
+        int* cnt = at<int>(L.ccnt);
+        unsigned short* list = at<unsigned short>(L.clist);
+        const int npx = P.npbc[0], npy = P.npbc[1], npz = P.npbc[2];
+        const int nw = L.nwords;
+        for (int base = warp * 32; base < natoms; base += T) {
+            const int j = base + lane;
+            const float4 p = (j < natoms) ? spos[j] : make_float4(0, 0, 0, 0);
+            int k = 0;
+            for (int iz = -npz; iz <= npz; iz++)
+                for (int iy = -npy; iy <= npy; iy++)
+                    for (int ix = -npx; ix <= npx; ix++) {
+                        if ((ix | iy | iz) == 0) continue;
+                        bool c = false;
+                        if (j < natoms && image_active(ix, iy, iz)) {
+                            const float3 sh = image_shift(lv, ix, iy, iz);
+                            const float qx = p.x + sh.x, qy = p.y + sh.y, qz = p.z + sh.z;
+                            const float gx = fmaxf(0.f, fmaxf(bbmin[0] - qx, qx - bbmax[0]));
+                            const float gy = fmaxf(0.f, fmaxf(bbmin[1] - qy, qy - bbmax[1]));
+                            const float gz = fmaxf(0.f, fmaxf(bbmin[2] - qz, qz - bbmax[2]));
+                            c = gx * gx + gy * gy + gz * gz < P.Rc2;
+                        }
+                        const uint32_t bal = __ballot_sync(0xffffffffu, c);
+                        if (lane == 0) words[k * nw + (base >> 5)] = bal;
+                        k++;
+                    }
+        }
+        __syncthreads();
+        for (int k = warp; k < L.nimg; k += L.nwarps) {
+            int run = 0;
+            for (int w0 = 0; w0 < nw; w0 += 32) {
+                const int w = w0 + lane;
+                const uint32_t m = (w < nw && 32 * w < natoms) ? words[k * nw + w] : 0u;
+                const int c = __popc(m);
+                int incl = c;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += t;
+                }
+                if (w < nw) pref[k * nw + w] = run + incl - c;
+                run += __shfl_sync(0xffffffffu, incl, 31);
+            }
+            if (lane == 0) cnt[k] = run;
+        }
+        __syncthreads();
+        for (int j = tid; j < natoms; j += T) {
+            const int w = j >> 5;
+            const uint32_t below = (1u << (j & 31)) - 1u;
+            for (int k = 0; k < L.nimg; k++) {
+                const uint32_t m = words[k * nw + w];
+                if ((m >> (j & 31)) & 1u) list[k * L.maxNA + pref[k * nw + w] + __popc(m & below)] = (unsigned short)j;
+            }
+        }
+        __syncthreads();
+    }
+
+    // pair sum of one atom (already shifted by the image) over j = sub, sub+S, ...
+    // Branch-free: excluded and out-of-range pairs get r^2 = 1e30, where every
+    // term underflows to zero except the shifted-force constant kq Q / r
+    // (< 1e-16 eV/A).  HB: the system has H-bond pseudo-charges (block-uniform).
+    // list (nullable): candidate atoms of a shifted image, ascending; else all atoms
+    template <bool HB>
+    __device__ __forceinline__ void pair_row(const float4* spos, const float4* sREQ, int sub, float4 Ri, float pxs,
+                                             float pys, float pzs, int e0, int e1, int e2, int e3, int e4,
+                                             const unsigned short* list, int ncand,
+                                             float& fx, float& fy, float& fz, float& ei) {
+        const bool CUT = P.Rc2 > 0.f;
+        const float Rc2 = CUT ? P.Rc2 : 3.0e38f, kq = P.kq_rc2;
+        const float rc = CUT ? sqrtf(1.f / kq) : 0.f;
+        const int n = list ? ncand : natoms;
+        for (int c = sub; c < n; c += S) {
+            const int j = list ? (int)list[c] : c;
+            const float4 pj = spos[j];
+            const float4 Rj = sREQ[j];
+            const float dx = pj.x - pxs, dy = pj.y - pys, dz = pj.z - pzs;
+            float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            const bool ex = (j == e0) | (j == e1) | (j == e2) | (j == e3) | (j == e4);
+            const bool ok = !ex && (r2 < Rc2);
+            if (COUNT && ok) npair++;
+            r2 = ok ? r2 : 1e30f;
+            const float ir = rsqrtf(r2);
+            const float ir2 = ir * ir;
+            const float R0 = Ri.x + Rj.x;
+            const float E0 = Ri.y * Rj.y;
+            const float Q = Ri.z * Rj.z;
+            const float Eel = Q * ir;
+            const float u2 = R0 * R0 * ir2;
+            const float u6 = u2 * u2 * u2;
+            const float vdW = u6 * E0;
+            const float H = HB ? u6 * vdW * fminf(Ri.w * Rj.w, 0.f) : 0.f;
+            float F = -fmaf(12.f * ir2, HB ? fmaf(u6 - 1.f, vdW, H) : (u6 - 1.f) * vdW, Eel * ir2);
+            F = fmaf(Q * kq, ir, F);
+            fx = fmaf(dx, F, fx); fy = fmaf(dy, F, fy); fz = fmaf(dz, F, fz);
+            if (ENERGY && ok) {
+                float e = fmaf(u6 - 2.f, vdW, Eel + H);
+                if (CUT) e += Q * kq * (r2 * ir - 2.f * rc);
+                ei += e;
+            }
+        }
+    }
+
     // ------------------------------------------------------------------ phase 1
     // returns this thread's energy contributions (only meaningful if ENERGY)
     __device__ void forces(double& Eb, double& Enb, double& Eg) {
@@ -169,7 +283,11 @@ struct Engine {
             const bool pbc = (flags & F_PBC) != 0;
             const int npx = pbc ? P.npbc[0] : 0, npy = pbc ? P.npbc[1] : 0, npz = pbc ? P.npbc[2] : 0;
             const int nxi = 2 * npx + 1, nyi = 2 * npy + 1;
-            const bool cut = P.Rc2 > 0.f;
+            const bool lists = L.nimg > 0;          // cutoff + PBC: candidate lists per shifted image
+            if (lists) build_candidates();
+            const int central = (npz * nyi + npy) * nxi + npx;
+            const unsigned short* clist = at<unsigned short>(L.clist);
+            const int* ccnt = at<int>(L.ccnt);
             const int nunits = natoms * S;
             for (int u0 = 0; u0 < nunits; u0 += T) {
                 const int u = u0 + tid;
@@ -194,34 +312,11 @@ struct Engine {
                                 const int e3 = (ngC.z == ipbc || !pbc) ? ng.z : -1;
                                 const int e4 = (ngC.w == ipbc || !pbc) ? ng.w : -1;
                                 float ei = 0.f;
-                                for (int j = sub; j < natoms; j += S) {
-                                    const float4 pj = spos[j];
-                                    const float4 Rj = sREQ[j];
-                                    const float dx = pj.x - pxs, dy = pj.y - pys, dz = pj.z - pzs;
-                                    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                                    const bool ex = (j == e0) | (j == e1) | (j == e2) | (j == e3) | (j == e4);
-                                    if (ex) continue;
-                                    if (cut && r2 >= P.Rc2) continue;
-                                    if (COUNT) npair++;
-                                    const float R0 = Ri.x + Rj.x;
-                                    const float E0 = Ri.y * Rj.y;
-                                    const float Q = Ri.z * Rj.z;
-                                    const float hw = fminf(Ri.w * Rj.w, 0.f);
-                                    float eij = 0.f;
-                                    float F = ljqh<ENERGY>(r2, R0, E0, Q, hw, eij);
-                                    if (cut) {
-                                        // shifted-force Coulomb: F_el(r) - F_el(Rc) along r
-                                        const float ir = rsqrtf(r2);
-                                        F = fmaf(Q * P.kq_rc2, ir, F);
-                                        if (ENERGY) {
-                                            const float r = r2 * ir;
-                                            const float rc = sqrtf(1.f / P.kq_rc2);
-                                            eij += Q * P.kq_rc2 * (r - 2.f * rc);
-                                        }
-                                    }
-                                    fx = fmaf(dx, F, fx); fy = fmaf(dy, F, fy); fz = fmaf(dz, F, fz);
-                                    if (ENERGY) ei += eij;
-                                }
+                                const int kimg = ipbc < central ? ipbc : ipbc - 1;
+                                const unsigned short* lst = (lists && ipbc != central) ? clist + kimg * L.maxNA : nullptr;
+                                const int ncand = lst ? ccnt[kimg] : 0;
+                                if (hasH) pair_row<true>(spos, sREQ, sub, Ri, pxs, pys, pzs, e0, e1, e2, e3, e4, lst, ncand, fx, fy, fz, ei);
+                                else pair_row<false>(spos, sREQ, sub, Ri, pxs, pys, pzs, e0, e1, e2, e3, e4, lst, ncand, fx, fy, fz, ei);
                                 if (ENERGY) e += (double)ei;
                             }
                 }
@@ -391,7 +486,7 @@ __global__ void __launch_bounds__(T) relax_kernel(Params P, Systems Y, const int
                                                   int* counter, int maxNA, int maxNN) {
     extern __shared__ __align__(16) char smem[];
     __shared__ int s_claim;
-    const SmemLayout L = smem_layout(maxNA, maxNN, T);
+    const SmemLayout L = smem_layout(maxNA, maxNN, T, P.Rc2 > 0.f ? shifted_images(P.flags, P.npbc) : 0);
     Engine<T, S, false, COUNT> E(P, Y, smem, L);
     while (true) {
         if (threadIdx.x == 0) s_claim = atomicAdd(counter, 1);
@@ -461,7 +556,7 @@ template <int T, int S, bool ENERGY>
 __global__ void __launch_bounds__(T) eval_kernel(Params P, Systems Y, const int* __restrict__ queue, int nqueue,
                                                  int maxNA, int maxNN) {
     extern __shared__ __align__(16) char smem[];
-    const SmemLayout L = smem_layout(maxNA, maxNN, T);
+    const SmemLayout L = smem_layout(maxNA, maxNN, T, P.Rc2 > 0.f ? shifted_images(P.flags, P.npbc) : 0);
     Engine<T, S, ENERGY> E(P, Y, smem, L);
     const int q = blockIdx.x;
     if (q >= nqueue) return;

@@ -165,11 +165,15 @@ __device__ __forceinline__ float eval_atom_slots(int ia, int natoms, int nnode, 
     return E;
 }
 
-// pair-sum inner loop over all j for (up to) two owned atoms, one image
-// One code path for every setting keeps the instruction footprint small (the
-// kernel is instruction-fetch bound otherwise): without a cutoff Rc2 is +inf
-// and kq 0, without H-bond pseudo-charges the H term multiplies by 0.
-template <int APL, bool ENERGY, bool COUNT>
+// pair-sum inner loop over all j for (up to) two owned atoms, one image.
+// One code path for cutoff / no cutoff keeps the instruction footprint small
+// (the kernel is instruction-fetch bound otherwise): without a cutoff Rc2 is
+// +inf and kq 0.  HB: the system has H-bond pseudo-charges (a warp-uniform
+// choice; without them the H term is identically 0 and is not evaluated).
+// Excluded and out-of-range pairs get r^2 = 1e30: every term then underflows
+// to zero except the shifted-force constant kq Q / r, below 1e-16 eV/A, so no
+// final select is needed.
+template <int APL, bool ENERGY, bool COUNT, bool HB>
 __device__ __forceinline__ void pair_image(const Params& P, int N, const float4* __restrict__ sp,
                                            const float4* __restrict__ sR, float3 p0, float3 p1, float4 R0i,
                                            float4 R1i, uint32_t m0lo, uint32_t m0hi, uint32_t m1lo, uint32_t m1hi,
@@ -196,10 +200,9 @@ __device__ __forceinline__ void pair_image(const Params& P, int N, const float4*
             const float u2 = R0 * R0 * ir2;
             const float u6 = u2 * u2 * u2;
             const float vdW = u6 * E0;
-            const float H = u6 * vdW * fminf(R0i.w * Rj.w, 0.f);
-            float F = -fmaf(12.f * ir2, fmaf(u6 - 1.f, vdW, H), Eel * ir2);
+            const float H = HB ? u6 * vdW * fminf(R0i.w * Rj.w, 0.f) : 0.f;
+            float F = -fmaf(12.f * ir2, HB ? fmaf(u6 - 1.f, vdW, H) : (u6 - 1.f) * vdW, Eel * ir2);
             F = fmaf(Q * kq, ir, F);
-            F = ok ? F : 0.f;
             f0.x = fmaf(dx, F, f0.x); f0.y = fmaf(dy, F, f0.y); f0.z = fmaf(dz, F, f0.z);
             if (ENERGY && ok) {
                 float e = fmaf(u6 - 2.f, vdW, Eel + H);
@@ -222,10 +225,9 @@ __device__ __forceinline__ void pair_image(const Params& P, int N, const float4*
             const float u2 = R0 * R0 * ir2;
             const float u6 = u2 * u2 * u2;
             const float vdW = u6 * E0;
-            const float H = u6 * vdW * fminf(R1i.w * Rj.w, 0.f);
-            float F = -fmaf(12.f * ir2, fmaf(u6 - 1.f, vdW, H), Eel * ir2);
+            const float H = HB ? u6 * vdW * fminf(R1i.w * Rj.w, 0.f) : 0.f;
+            float F = -fmaf(12.f * ir2, HB ? fmaf(u6 - 1.f, vdW, H) : (u6 - 1.f) * vdW, Eel * ir2);
             F = fmaf(Q * kq, ir, F);
-            F = ok ? F : 0.f;
             f1.x = fmaf(dx, F, f1.x); f1.y = fmaf(dy, F, f1.y); f1.z = fmaf(dz, F, f1.z);
             if (ENERGY && ok) {
                 float e = fmaf(u6 - 2.f, vdW, Eel + H);
@@ -378,7 +380,10 @@ struct WarpEngine {
                         if (APL == 2 && a1 < N) excl_mask(a1, sng[a1], sngC[a1], ipbc, pbc, m1lo, m1hi); else { m1lo = m1hi = ~0u; }
                         const float3 p0 = make_float3(q0.x - shx, q0.y - shy, q0.z - shz);
                         const float3 p1 = make_float3(q1.x - shx, q1.y - shy, q1.z - shz);
-                        pair_image<APL, ENERGY, COUNT>(P, N, sp, sR, p0, p1, Ri0, Ri1, m0lo, m0hi, m1lo, m1hi, f0, f1, e0, e1, npair);
+                        if (hasH)
+                            pair_image<APL, ENERGY, COUNT, true>(P, N, sp, sR, p0, p1, Ri0, Ri1, m0lo, m0hi, m1lo, m1hi, f0, f1, e0, e1, npair);
+                        else
+                            pair_image<APL, ENERGY, COUNT, false>(P, N, sp, sR, p0, p1, Ri0, Ri1, m0lo, m0hi, m1lo, m1hi, f0, f1, e0, e1, npair);
                     }
             if (ENERGY) Enb += 0.5 * ((double)e0 + (double)e1);
         }

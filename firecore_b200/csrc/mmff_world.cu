@@ -209,7 +209,7 @@ int config_bucket(Bucket& B, int kind, int apl, int T, int S) {
         fns[0] = relax_warp_fn(B.apl, false); fns[1] = relax_warp_fn(B.apl, true);
     } else {
         B.kind = 0; B.T = T; B.S = S;
-        B.smem = smem_layout(B.maxNA, B.maxNN, B.T).total;
+        B.smem = smem_layout(B.maxNA, B.maxNN, B.T, W.Rcut > 0 ? shifted_images(W.flags, W.npbc) : 0).total;
         fns[0] = relax_fn(B.T, B.S, false); fns[1] = relax_fn(B.T, B.S, true);
     }
     if (B.smem > dev_smem) return fail("system too large for shared memory: %d B > %d B", B.smem, dev_smem);
@@ -346,6 +346,7 @@ int mmff_sync(void) {
 
 int mmff_set_params(int flags, const int* nPBC, double Rcut, double alphaMorse, double FmaxNonBonded) {
     W.version++;
+    W.buckets_dirty = true;     // shared-memory size depends on the image set and the cutoff
     W.flags = flags;
     if (nPBC) for (int k = 0; k < 3; k++) W.npbc[k] = nPBC[k];
     W.Rcut = Rcut;

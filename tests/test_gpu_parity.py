@@ -94,6 +94,19 @@ def test_grid_build_vs_oracle(world, golden):
     world.grid_upload(golden["C"], grid_from_golden(golden))
 
 
+@pytest.mark.parametrize("hbond", [False, True])
+def test_uneven_pbc_cutoff_vs_oracle(world, golden, hbond):
+    """Molecules of 20..400 atoms in a 22.56 A cell with x,y images and a 10 A
+    cutoff: every size class, the CTA kernels' per-image candidate lists
+    (large molecules reach their own images) and both pair-loop variants
+    (with / without H-bond pseudo-charges)."""
+    sizes = [20, 33, 57, 64, 65, 120, 128, 129, 200, 256, 257, 330, 400]
+    b = S.make_systems(sizes, seed=11, topo_mode=1, sigma=0.1, cell=(22.56, 22.56, 40.0), hbond=hbond)
+    ferr, eerr = check_eval(world, b, grid_from_golden(golden), golden["C"], DEFAULT_FLAGS, npbc=(1, 1, 0), Rcut=10.0)
+    assert ferr.max() < FTOL, ferr
+    assert eerr.max() < ETOL, eerr
+
+
 def test_uneven_batch_vs_oracle(world, golden):
     sizes = [20, 33, 57, 64, 65, 120, 128, 129, 200, 256, 257, 400]
     b = S.make_systems(sizes, seed=3, topo_mode=1, sigma=0.1, cell=(11.28, 11.28, 40.0), npbc=(0, 0, 0))
