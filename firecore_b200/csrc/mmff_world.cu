@@ -192,6 +192,23 @@ int size_class(int na) {
     return 5;
 }
 
+// Raise a kernel's dynamic shared-memory limit to at least `bytes`.  The limit
+// is per function, and several buckets (or autotuner candidates) can share one
+// kernel instantiation, so it only ever grows.
+int set_smem_limit(void* fn, int bytes) {
+    static std::vector<std::pair<void*, int>> seen;
+    for (auto& e : seen) {
+        if (e.first != fn) continue;
+        if (bytes <= e.second) return 0;
+        CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        e.second = bytes;
+        return 0;
+    }
+    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    seen.emplace_back(fn, bytes);
+    return 0;
+}
+
 // launch configuration of a bucket whose systems are set: kind 1 = warp
 // engine (apl atoms per lane), kind 0 = CTA engine with T threads and S lanes
 // per atom in the pair sum.  Fills smem, grid; sets kernel attributes.
@@ -214,10 +231,10 @@ int config_bucket(Bucket& B, int kind, int apl, int T, int S) {
     }
     if (B.smem > dev_smem) return fail("system too large for shared memory: %d B > %d B", B.smem, dev_smem);
     if (!fns[0] || !fns[1]) return fail("no kernel for bucket (kind %d, T=%d, S=%d)", B.kind, B.T, B.S);
-    for (int f = 0; f < 2; f++) CK(cudaFuncSetAttribute(fns[f], cudaFuncAttributeMaxDynamicSharedMemorySize, B.smem));
+    for (int f = 0; f < 2; f++) if (set_smem_limit(fns[f], B.smem)) return -1;
     for (int e = 0; e < 2; e++) {
         void* ef = B.kind ? eval_warp_fn(B.apl, e) : eval_fn(B.T, B.S, e);
-        CK(cudaFuncSetAttribute(ef, cudaFuncAttributeMaxDynamicSharedMemorySize, B.smem));
+        if (set_smem_limit(ef, B.smem)) return -1;
     }
     int occ = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fns[0], B.T, B.smem));
@@ -593,7 +610,7 @@ int mmff_relax(int nstep_max, double Fconv, int conv_mode) {
         CK(cudaStreamBeginCapture(W.stream, cudaStreamCaptureModeThreadLocal));
         const int rc = enqueue_relax(P);
         const cudaError_t e = cudaStreamEndCapture(W.stream, &g);
-        if (rc) { if (g) cudaGraphDestroy(g); return -1; }
+        if (rc) { if (g) cudaGraphDestroy(g); cudaGetLastError(); return -1; }
         if (e != cudaSuccess) return fail("relax graph capture: %s", cudaGetErrorString(e));
         const cudaError_t ei = cudaGraphInstantiate(&W.gexec, g, 0);
         cudaGraphDestroy(g);

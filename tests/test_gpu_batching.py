@@ -16,6 +16,15 @@ def world():
     return World(0)
 
 
+@pytest.fixture(autouse=True)
+def _restore_launch_state(world):
+    """Graph mode and tuned launch shapes are library-wide: put them back."""
+    yield
+    world.set_graph(False)
+    for c in range(6):
+        world.lib.mmff_set_tuning(c, -1, 1, 0, 0)
+
+
 def uneven(world, golden, n=96, seed=5, lo=20, hi=300):
     grid = grid_from_golden(golden)
     sizes = S.loguniform_sizes(n, seed, lo, hi)
