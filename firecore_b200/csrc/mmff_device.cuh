@@ -101,6 +101,39 @@ __device__ __forceinline__ float ljqh(float r2, float R0, float E0, float Q, flo
     return -fmaf(12.f * ir2, fmaf(u6 - 1.f, vdW, H), Eel * ir2);
 }
 
+// scalar pair force F (f_i += d F with d = p_j - p_i) of one pair-image, the
+// arithmetic of the pair loops (rsqrt form of getLJQH, Forces.h:341-360, plus
+// the shifted-force Coulomb term); ok: inside the cutoff and not excluded.
+// Excluded / out-of-range pairs are evaluated at r^2 = 1e30, where every term
+// underflows to zero except kq Q / r (< 1e-16 eV/A).
+template <bool ENERGY, bool HB>
+__device__ __forceinline__ float pair_force(float dx, float dy, float dz, float4 Ri, float4 Rj, bool excl, float Rc2,
+                                            float kq, float rc, bool cut, bool& ok, float& e) {
+    float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    ok = !excl && (r2 < Rc2);
+    r2 = ok ? r2 : 1e30f;
+    const float ir = rsqrtf(r2);
+    const float ir2 = ir * ir;
+    const float R0 = Ri.x + Rj.x;
+    const float E0 = Ri.y * Rj.y;
+    const float Q = Ri.z * Rj.z;
+    const float Eel = Q * ir;
+    const float u2 = R0 * R0 * ir2;
+    const float u6 = u2 * u2 * u2;
+    const float vdW = u6 * E0;
+    const float H = HB ? u6 * vdW * fminf(Ri.w * Rj.w, 0.f) : 0.f;
+    float F = -fmaf(12.f * ir2, HB ? fmaf(u6 - 1.f, vdW, H) : (u6 - 1.f) * vdW, Eel * ir2);
+    F = fmaf(Q * kq, ir, F);
+    if (ENERGY) {
+        e = 0.f;
+        if (ok) {
+            e = fmaf(u6 - 2.f, vdW, Eel + H);
+            if (cut) e += Q * kq * (r2 * ir - 2.f * rc);
+        }
+    }
+    return F;
+}
+
 // ----- bonded terms (one node atom), MMFFsp3_loc::eval_atom
 struct BondedOut {
     float3 fa, fpi;
@@ -346,7 +379,8 @@ struct SmemLayout {
     int maxNA, maxNN, maxNV, nwarps, nimg, nwords;
     // offsets in bytes
     int pos, vel, fasm, fnb, fgrid, REQ, PLQ, ng, ngC, bk, apar, bL, bK, ksp, kpp, fng, red;
-    int cwords, cpref, ccnt, clist, total;     // per-image candidate lists (cutoff + PBC only)
+    int cwords, cpref, ccnt, clist;     // per-image candidate lists (cutoff + PBC only)
+    int facc, total;                    // fixed-point force sums of the central image [3 * maxNA] int64
 };
 
 // number of shifted (non-central) PBC images of the pair term
@@ -383,6 +417,7 @@ __host__ __device__ inline SmemLayout smem_layout(int maxNA, int maxNN, int T, i
     L.cpref = take(4 * nimg * L.nwords);    // exclusive prefix of their popcounts
     L.ccnt = take(4 * nimg);                // candidates per image
     L.clist = take(2 * nimg * maxNA);       // candidate atom indices per image, ascending
+    L.facc = take(8 * 3 * maxNA);
     L.total = o;
     return L;
 }

@@ -268,6 +268,123 @@ struct Engine {
         else pair_row<false>(spos, sREQ, sub, Ri, pxs, pys, pzs, e0, e1, e2, e3, e4, list, ncand, fx, fy, fz, ei);
     }
 
+    // ---- central image, each unordered pair once (Newton's third law) --------
+    // 32 x 32 atom tiles: the 32 lanes of a warp own the atoms i of block bi,
+    // the atoms j of block bj rotate through the lanes (lane l meets j-slot
+    // l + s at step s) and so does the reaction accumulator of the current j,
+    // which after 32 steps sits in lane j - 32 bj.  Diagonal tiles take steps
+    // 1..16 (s = 16 on lanes < 16 only) and return reactions by shuffle.  Tile
+    // sums reach the per-atom totals through 64-bit fixed-point shared-memory
+    // adds (2^-32 eV/A resolution): integer addition is associative, so the
+    // totals do not depend on which warp finishes first.
+    static constexpr float kFix = 4294967296.f;
+    __device__ __forceinline__ void fix_add(long long* a, float3 f) {
+        atomicAdd(reinterpret_cast<unsigned long long*>(a + 0), (unsigned long long)__float2ll_rn(f.x * kFix));
+        atomicAdd(reinterpret_cast<unsigned long long*>(a + 1), (unsigned long long)__float2ll_rn(f.y * kFix));
+        atomicAdd(reinterpret_cast<unsigned long long*>(a + 2), (unsigned long long)__float2ll_rn(f.z * kFix));
+    }
+
+    // own atom i of a tile: position, parameters and its bonded neighbours in
+    // the central cell (the excluded j); invalid slots exclude everything
+    struct TileAtom { float4 p, R; int e1, e2, e3, e4; bool v; };
+    __device__ __forceinline__ TileAtom tile_atom(int i, const float4* spos, const float4* sREQ, bool pbc, int central) {
+        TileAtom t;
+        t.v = i < natoms;
+        const int ic = t.v ? i : 0;
+        t.p = spos[ic]; t.R = sREQ[ic];
+        const int4 ng = at<int4>(L.ng)[ic], ngC = at<int4>(L.ngC)[ic];
+        t.e1 = (ngC.x == central || !pbc) ? ng.x : -1;
+        t.e2 = (ngC.y == central || !pbc) ? ng.y : -1;
+        t.e3 = (ngC.z == central || !pbc) ? ng.z : -1;
+        t.e4 = (ngC.w == central || !pbc) ? ng.w : -1;
+        return t;
+    }
+
+    template <bool HB>
+    __device__ void off_tile(int bi, int bj, const float4* spos, const float4* sREQ, bool pbc, int central,
+                             long long* facc, float& ec) {
+        const bool CUT = P.Rc2 > 0.f;
+        const float Rc2 = CUT ? P.Rc2 : 3.0e38f, kq = P.kq_rc2;
+        const float rc = CUT ? sqrtf(1.f / kq) : 0.f;
+        const int i = bi * 32 + lane;
+        const TileAtom a = tile_atom(i, spos, sREQ, pbc, central);
+        float3 fi = make_float3(0.f, 0.f, 0.f), rj = make_float3(0.f, 0.f, 0.f);
+        bool ok;
+        float e = 0.f;
+#pragma unroll 1
+        for (int s = 0; s < 32; s++) {
+            const int j = bj * 32 + ((lane + s) & 31);
+            const bool vj = j < natoms;
+            const float4 pj = spos[vj ? j : 0], Rj = sREQ[vj ? j : 0];
+            const bool excl = !a.v || !vj || j == a.e1 || j == a.e2 || j == a.e3 || j == a.e4;
+            const float dx = pj.x - a.p.x, dy = pj.y - a.p.y, dz = pj.z - a.p.z;
+            const float F = pair_force<ENERGY, HB>(dx, dy, dz, a.R, Rj, excl, Rc2, kq, rc, CUT, ok, e);
+            fi.x = fmaf(dx, F, fi.x); fi.y = fmaf(dy, F, fi.y); fi.z = fmaf(dz, F, fi.z);
+            rj.x = fmaf(-dx, F, rj.x); rj.y = fmaf(-dy, F, rj.y); rj.z = fmaf(-dz, F, rj.z);
+            if (ENERGY) ec += e;
+            if (COUNT && ok) npair += 2;
+            const int nxt = (lane + 1) & 31;
+            rj.x = __shfl_sync(0xffffffffu, rj.x, nxt);
+            rj.y = __shfl_sync(0xffffffffu, rj.y, nxt);
+            rj.z = __shfl_sync(0xffffffffu, rj.z, nxt);
+        }
+        if (a.v) fix_add(facc + 3 * i, fi);
+        const int jo = bj * 32 + lane;
+        if (jo < natoms) fix_add(facc + 3 * jo, rj);
+    }
+
+    template <bool HB>
+    __device__ void diag_tile(int b, const float4* spos, const float4* sREQ, bool pbc, int central, long long* facc,
+                              float& ec) {
+        const bool CUT = P.Rc2 > 0.f;
+        const float Rc2 = CUT ? P.Rc2 : 3.0e38f, kq = P.kq_rc2;
+        const float rc = CUT ? sqrtf(1.f / kq) : 0.f;
+        const int i = b * 32 + lane;
+        const TileAtom a = tile_atom(i, spos, sREQ, pbc, central);
+        float3 fi = make_float3(0.f, 0.f, 0.f);
+        bool ok;
+        float e = 0.f;
+#pragma unroll 1
+        for (int s = 1; s <= 16; s++) {
+            const int j = b * 32 + ((lane + s) & 31);
+            const bool vj = j < natoms;
+            const float4 pj = spos[vj ? j : 0], Rj = sREQ[vj ? j : 0];
+            const bool half = (s < 16) || (lane < 16);
+            const bool excl = !a.v || !vj || !half || j == a.e1 || j == a.e2 || j == a.e3 || j == a.e4;
+            const float dx = pj.x - a.p.x, dy = pj.y - a.p.y, dz = pj.z - a.p.z;
+            const float F = pair_force<ENERGY, HB>(dx, dy, dz, a.R, Rj, excl, Rc2, kq, rc, CUT, ok, e);
+            fi.x = fmaf(dx, F, fi.x); fi.y = fmaf(dy, F, fi.y); fi.z = fmaf(dz, F, fi.z);
+            if (ENERGY) ec += e;
+            if (COUNT && ok) npair += 2;
+            const int src = (lane - s) & 31;     // the lane whose partner this lane's atom was
+            fi.x += __shfl_sync(0xffffffffu, -dx * F, src);
+            fi.y += __shfl_sync(0xffffffffu, -dy * F, src);
+            fi.z += __shfl_sync(0xffffffffu, -dz * F, src);
+        }
+        if (a.v) fix_add(facc + 3 * i, fi);
+    }
+
+    // work units: each off-diagonal tile, and pairs of diagonal tiles (equal
+    // cost), dealt round-robin to the warps
+    template <bool HB>
+    __device__ void central_tiles(const float4* spos, const float4* sREQ, bool pbc, int central, long long* facc,
+                                  float& ec) {
+        const int B = (natoms + 31) >> 5;
+        const int noff = B * (B - 1) / 2;
+        const int nunits = noff + ((B + 1) >> 1);
+        for (int u = warp; u < nunits; u += L.nwarps) {
+            if (u < noff) {
+                int bi = 0, rem = u;
+                while (rem >= B - 1 - bi) { rem -= B - 1 - bi; bi++; }
+                off_tile<HB>(bi, bi + 1 + rem, spos, sREQ, pbc, central, facc, ec);
+            } else {
+                const int d = 2 * (u - noff);
+                diag_tile<HB>(d, spos, sREQ, pbc, central, facc, ec);
+                if (d + 1 < B) diag_tile<HB>(d + 1, spos, sREQ, pbc, central, facc, ec);
+            }
+        }
+    }
+
     // ------------------------------------------------------------------ phase 1
     // returns this thread's energy contributions (only meaningful if ENERGY)
     __device__ void forces(double& Eb, double& Enb, double& Eg) {
@@ -306,38 +423,56 @@ struct Engine {
             const int central = (npz * nyi + npy) * nxi + npx;
             const unsigned short* clist = at<unsigned short>(L.clist);
             const int* ccnt = at<int>(L.ccnt);
-            // pass 1: every atom against all atoms of the central image (and,
-            // without lists, of every image the bounding-box test keeps)
-            const int nunits = natoms * S;
-            for (int u0 = 0; u0 < nunits; u0 += T) {
-                const int u = u0 + tid;
-                const int i = u / S, sub = u % S;
-                float fx = 0.f, fy = 0.f, fz = 0.f;
-                double e = 0.0;
-                if (i < natoms) {
-                    const float4 pi = spos[i];
-                    const float4 Ri = sREQ[i];
-                    const int4 ng = sng[i], ngC = sngC[i];
-                    for (int iz = -npz; iz <= npz; iz++)
-                        for (int iy = -npy; iy <= npy; iy++)
-                            for (int ix = -npx; ix <= npx; ix++) {
-                                const int ipbc = ((iz + npz) * nyi + (iy + npy)) * nxi + (ix + npx);
-                                if (lists && ipbc != central) continue;
-                                if (!image_active(ix, iy, iz)) continue;
-                                float ei = 0.f;
-                                pair_image_row(spos, sREQ, i, sub, pi, Ri, ng, ngC, pbc, ipbc, ix, iy, iz, nullptr, 0, fx, fy, fz, ei);
-                                if (ENERGY) e += (double)ei;
-                            }
-                }
-                // reduce over the S lanes of atom i
+            // central image: every unordered pair once, into fixed-point sums
+            long long* facc = at<long long>(L.facc);
+            for (int a = tid; a < 3 * natoms; a += T) facc[a] = 0;
+            __syncthreads();
+            {
+                float ec = 0.f;
+                if (hasH) central_tiles<true>(spos, sREQ, pbc, central, facc, ec);
+                else central_tiles<false>(spos, sREQ, pbc, central, facc, ec);
+                if (ENERGY) Enb += (double)ec;
+            }
+            __syncthreads();
+            for (int a = tid; a < natoms; a += T)
+                fnb[a] = make_float4((float)facc[3 * a] * (1.f / kFix), (float)facc[3 * a + 1] * (1.f / kFix),
+                                     (float)facc[3 * a + 2] * (1.f / kFix), 0.f);
+            // without candidate lists: the other images of the bounding-box test,
+            // ordered pairs (i, j + shift), S lanes per atom
+            if (!lists && (npx | npy | npz)) {
+                __syncthreads();
+                const int nunits = natoms * S;
+                for (int u0 = 0; u0 < nunits; u0 += T) {
+                    const int u = u0 + tid;
+                    const int i = u / S, sub = u % S;
+                    float fx = 0.f, fy = 0.f, fz = 0.f;
+                    double e = 0.0;
+                    if (i < natoms) {
+                        const float4 pi = spos[i];
+                        const float4 Ri = sREQ[i];
+                        const int4 ng = sng[i], ngC = sngC[i];
+                        for (int iz = -npz; iz <= npz; iz++)
+                            for (int iy = -npy; iy <= npy; iy++)
+                                for (int ix = -npx; ix <= npx; ix++) {
+                                    const int ipbc = ((iz + npz) * nyi + (iy + npy)) * nxi + (ix + npx);
+                                    if (ipbc == central || !image_active(ix, iy, iz)) continue;
+                                    float ei = 0.f;
+                                    pair_image_row(spos, sREQ, i, sub, pi, Ri, ng, ngC, pbc, ipbc, ix, iy, iz, nullptr, 0, fx, fy, fz, ei);
+                                    if (ENERGY) e += (double)ei;
+                                }
+                    }
 #pragma unroll
-                for (int o = S / 2; o > 0; o >>= 1) {
-                    fx += __shfl_xor_sync(0xffffffffu, fx, o);
-                    fy += __shfl_xor_sync(0xffffffffu, fy, o);
-                    fz += __shfl_xor_sync(0xffffffffu, fz, o);
+                    for (int o = S / 2; o > 0; o >>= 1) {
+                        fx += __shfl_xor_sync(0xffffffffu, fx, o);
+                        fy += __shfl_xor_sync(0xffffffffu, fy, o);
+                        fz += __shfl_xor_sync(0xffffffffu, fz, o);
+                    }
+                    if (i < natoms && sub == 0) {
+                        const float4 a = fnb[i];
+                        fnb[i] = make_float4(a.x + fx, a.y + fy, a.z + fz, 0.f);
+                    }
+                    if (ENERGY) Enb += 0.5 * e;
                 }
-                if (i < natoms && sub == 0) fnb[i] = make_float4(fx, fy, fz, 0.f);
-                if (ENERGY) Enb += 0.5 * e;
             }
             // pass 2: each shifted image, its candidate atoms j against the
             // candidate atoms i of the opposite image (the atoms within the

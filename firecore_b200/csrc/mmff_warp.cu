@@ -239,36 +239,6 @@ __device__ __forceinline__ void pair_image(const Params& P, int N, const float4*
     }
 }
 
-// scalar pair force F (f_i += d F with d = p_j - p_i) of one pair-image, the
-// same arithmetic as pair_image; ok: inside the cutoff and not excluded
-template <bool ENERGY, bool HB>
-__device__ __forceinline__ float pair_force(float dx, float dy, float dz, float4 Ri, float4 Rj, bool excl, float Rc2,
-                                            float kq, float rc, bool cut, bool& ok, float& e) {
-    float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-    ok = !excl && (r2 < Rc2);
-    r2 = ok ? r2 : 1e30f;
-    const float ir = rsqrtf(r2);
-    const float ir2 = ir * ir;
-    const float R0 = Ri.x + Rj.x;
-    const float E0 = Ri.y * Rj.y;
-    const float Q = Ri.z * Rj.z;
-    const float Eel = Q * ir;
-    const float u2 = R0 * R0 * ir2;
-    const float u6 = u2 * u2 * u2;
-    const float vdW = u6 * E0;
-    const float H = HB ? u6 * vdW * fminf(Ri.w * Rj.w, 0.f) : 0.f;
-    float F = -fmaf(12.f * ir2, HB ? fmaf(u6 - 1.f, vdW, H) : (u6 - 1.f) * vdW, Eel * ir2);
-    F = fmaf(Q * kq, ir, F);
-    if (ENERGY) {
-        e = 0.f;
-        if (ok) {
-            e = fmaf(u6 - 2.f, vdW, Eel + H);
-            if (cut) e += Q * kq * (r2 * ir - 2.f * rc);
-        }
-    }
-    return F;
-}
-
 // Central-image pairs, each unordered pair once (Newton's third law).  Lane l
 // owns atoms A = l and B = l + 32; at rotation step s it meets the atoms of
 // lane p = l + s (mod 32): (A, A') and (B, B') for s = 1..15 (s = 16: lanes
