@@ -278,6 +278,10 @@ struct Engine {
     // adds (2^-32 eV/A resolution): integer addition is associative, so the
     // totals do not depend on which warp finishes first.
     static constexpr float kFix = 4294967296.f;
+#ifndef MMFF_TILE_UNROLL
+#define MMFF_TILE_UNROLL 1
+#endif
+    static constexpr int kTileUnroll = MMFF_TILE_UNROLL;   // tile-step unrolling (build option)
     __device__ __forceinline__ void fix_add(long long* a, float3 f) {
         atomicAdd(reinterpret_cast<unsigned long long*>(a + 0), (unsigned long long)__float2ll_rn(f.x * kFix));
         atomicAdd(reinterpret_cast<unsigned long long*>(a + 1), (unsigned long long)__float2ll_rn(f.y * kFix));
@@ -311,7 +315,7 @@ struct Engine {
         float3 fi = make_float3(0.f, 0.f, 0.f), rj = make_float3(0.f, 0.f, 0.f);
         bool ok;
         float e = 0.f;
-#pragma unroll 1
+#pragma unroll kTileUnroll
         for (int s = 0; s < 32; s++) {
             const int j = bj * 32 + ((lane + s) & 31);
             const bool vj = j < natoms;
@@ -344,7 +348,7 @@ struct Engine {
         float3 fi = make_float3(0.f, 0.f, 0.f);
         bool ok;
         float e = 0.f;
-#pragma unroll 1
+#pragma unroll kTileUnroll
         for (int s = 1; s <= 16; s++) {
             const int j = b * 32 + ((lane + s) & 31);
             const bool vj = j < natoms;

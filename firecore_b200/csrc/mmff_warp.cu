@@ -275,7 +275,11 @@ __device__ __forceinline__ void central_pairs(const Params& P, int N, int lane, 
         if (ENERGY) ec += e;
         if (COUNT && ok) np += 2;
     }
-#pragma unroll 1
+#ifndef MMFF_CENTRAL_UNROLL
+#define MMFF_CENTRAL_UNROLL 1
+#endif
+    constexpr int kUnroll = MMFF_CENTRAL_UNROLL;      // rotation-step unrolling (build option)
+#pragma unroll kUnroll
     for (int s = 1; s <= 16; s++) {
         const int p = (lane + s) & 31;
         const int src = (lane - s) & 31;      // lane whose partner is this lane
