@@ -41,10 +41,11 @@ RCUT = 10.0
 FLIM = 10.0
 PAIR_FLOPS = 32          # algorithmic FP32 flops per pair-image (both directions counted)
 GRID_BYTES = 1024        # 64 float4 gathers per atom B-spline sample
-# DRAM bytes (read + write) per system-step of the warp-engine relax kernel,
-# from the ncu capture in profiles/relax_warp_kernel_4096x60.md (86.5 MB over
-# 4096 systems x 200 steps); scaled by the system-steps of a launch
-DRAM_BYTES_PER_SYSTEM_STEP = 105.6
+# DRAM bytes (read + write) per system-step of the relax kernel the autotuner
+# picks for this workload, from the ncu capture in
+# profiles/relax_kernel_cta_4096x60.md (93.3 MB over 4096 systems x 200 steps);
+# scaled by the system-steps of a launch
+DRAM_BYTES_PER_SYSTEM_STEP = 113.9
 
 
 def env_rank():

@@ -86,12 +86,29 @@ __device__ __forceinline__ float3 operator*(float3 a, float f) { return make_flo
 __device__ __forceinline__ float dot3(float3 a, float3 b) { return fmaf(a.x, b.x, fmaf(a.y, b.y, a.z * b.z)); }
 __device__ __forceinline__ float3 fma3(float3 a, float f, float3 c) { return make_float3(fmaf(a.x, f, c.x), fmaf(a.y, f, c.y), fmaf(a.z, f, c.z)); }
 
+// image index c (NBFF.h:42 ordering: x fastest, then y, then z) -> shift
+// in lattice units.  Quotients by the small image counts go through a float
+// reciprocal: (c + 1/2) / n stays >= 1/(2n) away from an integer, far beyond
+// the 2-ulp error of __fdividef, so the integer parts are exact.
+__device__ __forceinline__ float3 image_cell(int c, int npx, int npy, int npz) {
+    const int nx = 2 * npx + 1, ny = 2 * npy + 1;
+    const int q = (int)__fdividef((float)c + 0.5f, (float)nx);
+    const int r = (int)__fdividef((float)q + 0.5f, (float)ny);
+    return make_float3((float)(c - q * nx - npx), (float)(q - r * ny - npy), (float)(r - npz));
+}
+
+// i mod n into [0, n) for grid indices (same float-reciprocal argument)
+__device__ __forceinline__ int wrap_index(int i, int n) {
+    const int q = (int)floorf(__fdividef((float)i + 0.5f, (float)n));
+    return i - q * n;
+}
+
 // Forces.h:341 getLJQH with undamped Coulomb; REQ holds the pair-mixed values with
 // Q = k_e*Qi*Qj.  Returns the scalar F with f = dp * F (the reference's -F).
 template <bool ENERGY>
 __device__ __forceinline__ float ljqh(float r2, float R0, float E0, float Q, float hw, float& E) {
-    const float ir2 = 1.0f / r2;
-    const float ir = sqrtf(ir2);
+    const float ir = rsqrtf(r2);
+    const float ir2 = ir * ir;
     const float Eel = Q * ir;
     const float u2 = R0 * R0 * ir2;
     const float u6 = u2 * u2 * u2;
@@ -151,7 +168,7 @@ __device__ __forceinline__ void eval_atom(int ia, int natoms, int nnode, int fla
     float3 fa = make_float3(0, 0, 0), fpi = make_float3(0, 0, 0);
     float3 fbs[4], fps[4];
     float3 hf[4];
-    float he[4];
+    float he[4], hl[4];
     float E = 0.f;
     const int ings[4] = {ng.x, ng.y, ng.z, ng.w};
     const int ingC[4] = {ngC.x, ngC.y, ngC.z, ngC.w};
@@ -160,7 +177,7 @@ __device__ __forceinline__ void eval_atom(int ia, int natoms, int nnode, int fla
     const float Kspa[4] = {ksp.x, ksp.y, ksp.z, ksp.w};
     const float Kppa[4] = {kpp.x, kpp.y, kpp.z, kpp.w};
 #pragma unroll
-    for (int i = 0; i < 4; i++) { fbs[i] = make_float3(0, 0, 0); fps[i] = make_float3(0, 0, 0); hf[i] = make_float3(0, 0, 1); he[i] = 1.f; }
+    for (int i = 0; i < 4; i++) { fbs[i] = make_float3(0, 0, 0); fps[i] = make_float3(0, 0, 0); hf[i] = make_float3(0, 0, 1); he[i] = 1.f; hl[i] = 1.f; }
     int nb = 0;
 #pragma unroll
     for (int i = 0; i < 4; i++) {
@@ -171,16 +188,17 @@ __device__ __forceinline__ void eval_atom(int ia, int natoms, int nnode, int fla
         if (flags & F_PBC) {
             // shift of image ingC (NBFF.h:42 ordering: iz outer, iy, ix inner)
             const int c = ingC[i];
-            const int nx = 2 * npx + 1, ny = 2 * npy + 1;
-            const float ix = (float)(c % nx - npx), iy = (float)((c / nx) % ny - npy), iz = (float)(c / (nx * ny) - npz);
+            const float3 cell = image_cell(c, npx, npy, npz);
+            const float ix = cell.x, iy = cell.y, iz = cell.z;
             h.x += lv[0] * ix + lv[3] * iy + lv[6] * iz;
             h.y += lv[1] * ix + lv[4] * iy + lv[7] * iz;
             h.z += lv[2] * ix + lv[5] * iy + lv[8] * iz;
         }
-        const float l = sqrtf(dot3(h, h));
-        const float il = 1.0f / l;
+        const float l2 = dot3(h, h);
+        const float il = rsqrtf(l2);
+        const float l = l2 * il;
         h = h * il;
-        hf[i] = h; he[i] = il;
+        hf[i] = h; he[i] = il; hl[i] = l;
         if (ia < ing) {
             if (flags & F_BONDS) {
                 const float dl = l - bLa[i];
@@ -249,7 +267,7 @@ __device__ __forceinline__ void eval_atom(int ia, int natoms, int nnode, int fla
                 if (ENERGY) E += ssK * (1.f - csx);
                 float fr = -ssK * csy;
                 c2 *= -2.f;
-                fr = fr / (4.f * c * s);
+                fr = __fdividef(fr, 4.f * c * s);
                 const float fr1 = fr * he[i];
                 const float fr2 = fr * he[j];
                 float3 f1 = make_float3(h.x * fr1 + hf[i].x * (fr1 * c2), h.y * fr1 + hf[i].y * (fr1 * c2), h.z * fr1 + hf[i].z * (fr1 * c2));
@@ -259,7 +277,7 @@ __device__ __forceinline__ void eval_atom(int ia, int natoms, int nnode, int fla
                     const int ing = ings[i], jng = ings[j];
                     const float4 Ri = sREQ[ing], Rj = sREQ[jng];
                     const float hw = fminf(Ri.w * Rj.w, 0.f);
-                    const float3 dp = hf[j] * (1.f / he[j]) - hf[i] * (1.f / he[i]);
+                    const float3 dp = hf[j] * hl[j] - hf[i] * hl[i];
                     float e;
                     const float F = ljqh<ENERGY>(dot3(dp, dp), Ri.x + Rj.x, Ri.y * Rj.y, Ri.z * Rj.z, hw, e);
                     float3 fij = dp * F;
@@ -301,8 +319,8 @@ __device__ __forceinline__ float4 grid_slice(const float4* __restrict__ G, int n
     if (u.y < 0.f) iy--;
     const float tx = u.x - (float)ix, ty = u.y - (float)iy, tz = u.z - (float)iz;
     iz = min(max(iz, 3), nz - 5);
-    ix = ix - 1; ix %= nx; if (ix < 0) ix += nx;
-    iy = iy - 1; iy %= ny; if (iy < 0) iy += ny;
+    ix = wrap_index(ix - 1, nx);
+    iy = wrap_index(iy - 1, ny);
     // x index of this slice with periodic wrap (Bspline.h:36-53 choose_inds_pbc)
     int xa = ix + a; if (xa >= nx) xa -= nx;
     const float4 bz = bs_basis(tz), dz = bs_dbasis(tz);
@@ -340,8 +358,8 @@ __device__ __forceinline__ float4 grid_atom(const Params& P, float3 u, float4 PL
     if (u.y < 0.f) iy--;
     const float tx = u.x - (float)ix, ty = u.y - (float)iy, tz = u.z - (float)iz;
     iz = min(max(iz, 3), nz - 5);
-    ix = ix - 1; ix %= nx; if (ix < 0) ix += nx;
-    iy = iy - 1; iy %= ny; if (iy < 0) iy += ny;
+    ix = wrap_index(ix - 1, nx);
+    iy = wrap_index(iy - 1, ny);
     const float4 bz = bs_basis(tz), dz = bs_dbasis(tz);
     const float4 by = bs_basis(ty), dy = bs_dbasis(ty);
     const float4 bx = bs_basis(tx), dx = bs_dbasis(tx);

@@ -671,8 +671,24 @@ struct Engine {
 
 // ---------------------------------------------------------------------------
 // Persistent relaxation: claims systems from queue[] via counter.
+// resident CTAs per SM the register allocation of the relax kernel targets,
+// per thread count (build options; without a target ptxas caps at 128
+// registers and spills)
+#ifndef MMFF_MINB_T64
+#define MMFF_MINB_T64 8
+#endif
+#ifndef MMFF_MINB_T128
+#define MMFF_MINB_T128 4
+#endif
+#ifndef MMFF_MINB_T256
+#define MMFF_MINB_T256 2
+#endif
+template <int T> constexpr int relax_min_blocks() {
+    return T == 64 ? MMFF_MINB_T64 : T == 128 ? MMFF_MINB_T128 : T == 256 ? MMFF_MINB_T256 : 1;
+}
+
 template <int T, int S, bool COUNT>
-__global__ void __launch_bounds__(T) relax_kernel(Params P, Systems Y, const int* __restrict__ queue, int nqueue,
+__global__ void __launch_bounds__(T, relax_min_blocks<T>()) relax_kernel(Params P, Systems Y, const int* __restrict__ queue, int nqueue,
                                                   int* counter, int maxNA, int maxNN) {
     extern __shared__ __align__(16) char smem[];
     __shared__ int s_claim;

@@ -49,13 +49,13 @@ __device__ __forceinline__ float eval_atom_slots(int ia, int natoms, int nnode, 
     const float4 apar = *gap;
     float3 fa = make_float3(0, 0, 0), fpi = make_float3(0, 0, 0);
     float3 hf[4];
-    float he[4];
+    float he[4], hl[4];
     float E = 0.f;
     const int ings[4] = {ng.x, ng.y, ng.z, ng.w};
     const int ingC[4] = {ngC.x, ngC.y, ngC.z, ngC.w};
     auto addslot = [](float4* slot, float3 v) { float4 t = *slot; t.x += v.x; t.y += v.y; t.z += v.z; *slot = t; };
 #pragma unroll
-    for (int i = 0; i < 4; i++) { fbs[i] = make_float4(0, 0, 0, 0); fps[i] = make_float4(0, 0, 0, 0); hf[i] = make_float3(0, 0, 1); he[i] = 1.f; }
+    for (int i = 0; i < 4; i++) { fbs[i] = make_float4(0, 0, 0, 0); fps[i] = make_float4(0, 0, 0, 0); hf[i] = make_float3(0, 0, 1); he[i] = 1.f; hl[i] = 1.f; }
     int nb = 0;
 #pragma unroll
     for (int i = 0; i < 4; i++) {
@@ -65,16 +65,17 @@ __device__ __forceinline__ float eval_atom_slots(int ia, int natoms, int nnode, 
         float3 h = f3(sp[ing]) - pa;
         if (flags & F_PBC) {
             const int c = ingC[i];
-            const int nx = 2 * npx + 1, ny = 2 * npy + 1;
-            const float ix = (float)(c % nx - npx), iy = (float)((c / nx) % ny - npy), iz = (float)(c / (nx * ny) - npz);
+            const float3 cell = image_cell(c, npx, npy, npz);
+            const float ix = cell.x, iy = cell.y, iz = cell.z;
             h.x += lv[0] * ix + lv[3] * iy + lv[6] * iz;
             h.y += lv[1] * ix + lv[4] * iy + lv[7] * iz;
             h.z += lv[2] * ix + lv[5] * iy + lv[8] * iz;
         }
-        const float l = sqrtf(dot3(h, h));
-        const float il = 1.0f / l;
+        const float l2 = dot3(h, h);
+        const float il = rsqrtf(l2);
+        const float l = l2 * il;
         h = h * il;
-        hf[i] = h; he[i] = il;
+        hf[i] = h; he[i] = il; hl[i] = l;
         if (ia < ing) {
             if (flags & F_BONDS) {
                 const float dl = l - gbL[i];
@@ -139,7 +140,7 @@ __device__ __forceinline__ float eval_atom_slots(int ia, int natoms, int nnode, 
                 if (ENERGY) E += ssK * (1.f - csx);
                 float fr = -ssK * csy;
                 c2 *= -2.f;
-                fr = fr / (4.f * c * s);
+                fr = __fdividef(fr, 4.f * c * s);
                 const float fr1 = fr * he[i];
                 const float fr2 = fr * he[j];
                 float3 f1 = make_float3(h.x * fr1 + hf[i].x * (fr1 * c2), h.y * fr1 + hf[i].y * (fr1 * c2), h.z * fr1 + hf[i].z * (fr1 * c2));
@@ -147,7 +148,7 @@ __device__ __forceinline__ float eval_atom_slots(int ia, int natoms, int nnode, 
                 fa = fa - (f1 + f2);
                 if (flags & F_SUB_ANGLE_NB) {
                     const float4 Ri = sREQ[ings[i]], Rj = sREQ[ings[j]];
-                    const float3 dp = hf[j] * (1.f / he[j]) - hf[i] * (1.f / he[i]);
+                    const float3 dp = hf[j] * hl[j] - hf[i] * hl[i];
                     float e;
                     const float F = ljqh<ENERGY>(dot3(dp, dp), Ri.x + Rj.x, Ri.y * Rj.y, Ri.z * Rj.z, fminf(Ri.w * Rj.w, 0.f), e);
                     float3 fij = dp * F;
