@@ -1,5 +1,5 @@
-// mmff_peaks.cu -- measured denominators for the roofline fractions that
-// have no published or driver-measured figure on this GPU:
+// mmff_peaks.cu -- measured denominators for the roofline fractions for
+// which no measured peak of this GPU is otherwise available:
 //   * FP32 CUDA-core FMA throughput: independent FFMA chains on every SM,
 //   * L2 read bandwidth: float4 sweeps over a buffer that stays L2-resident.
 #include <cuda_runtime.h>

@@ -167,7 +167,7 @@ def test_trained_proposal_gains_over_untrained(world, golden):
     world.upload(train)
     prop = L.Proposal()
     F, T = L.trajectory_dataset(world, prop, train, snapshots=(0, 10, 50), nstep_max=1500)
-    assert len(F) > 1000
+    assert len(F) > 500
     mean, std = F.mean(0), F.std(0) + 1e-6
     scale = float(math.sqrt((T ** 2).mean()))
     test = S.make_systems([24] * 128, seed=22, topo_mode=1, sigma=0.15, cell=(11.28, 11.28, 40.0))

@@ -94,6 +94,30 @@ def test_grid_build_vs_oracle(world, golden):
     world.grid_upload(golden["C"], grid_from_golden(golden))
 
 
+def check_eval_components(world, b, grid, C, npbc, Rcut):
+    """Per-system FP32 force error against the summed magnitude of the force
+    components (bonded incl. 1-3 subtraction, pairs, grid) and energy error
+    against the summed component energies.  The generated molecules have close
+    non-bonded contacts whose pair forces (hundreds of eV/A) cancel against the
+    1-3 subtraction of the angle terms; FP32 rounding scales with those terms,
+    not with the small net force."""
+    world.set_params(flags=DEFAULT_FLAGS, npbc=npbc, Rcut=Rcut)
+    world.upload(b)
+    F, E = world.eval(True)
+    pos = world.state()["pos"]
+    mk = lambda fl: O.make_params(grid, flags=fl, npbc=npbc, Rcut=Rcut)
+    Fo, Eo = O.eval_forces(b, mk(DEFAULT_FLAGS), C, pos=pos)
+    comp = np.zeros_like(Fo)
+    for fl in (DEFAULT_FLAGS & ~(GRID | NONBONDED), NONBONDED | (DEFAULT_FLAGS & PBC), GRID | (DEFAULT_FLAGS & PBC)):
+        Fc, _ = O.eval_forces(b, mk(fl), C, pos=pos)
+        comp += np.abs(Fc)
+    a, n, v = b.offsets()
+    ferr = np.array([np.abs(F[v[s]:v[s + 1]] - Fo[v[s]:v[s + 1]]).max() / comp[v[s]:v[s + 1]].max()
+                     for s in range(b.nsys)])
+    eerr = np.abs(E - Eo).max(1) / np.maximum(np.abs(Eo[:, :3]).sum(1), 1e-9)
+    return ferr, eerr
+
+
 @pytest.mark.parametrize("hbond", [False, True])
 def test_uneven_pbc_cutoff_vs_oracle(world, golden, hbond):
     """Molecules of 20..400 atoms in a 22.56 A cell with x,y images and a 10 A
@@ -105,29 +129,15 @@ def test_uneven_pbc_cutoff_vs_oracle(world, golden, hbond):
     is measured against the summed magnitude of the force components."""
     sizes = [20, 33, 57, 64, 65, 120, 128, 129, 200, 256, 257, 330, 400]
     b = S.make_systems(sizes, seed=11, topo_mode=1, sigma=0.1, cell=(22.56, 22.56, 40.0), hbond=hbond)
-    grid = grid_from_golden(golden)
-    world.set_params(flags=DEFAULT_FLAGS, npbc=(1, 1, 0), Rcut=10.0)
-    world.upload(b)
-    F, E = world.eval(True)
-    pos = world.state()["pos"]
-    Fo, Eo = O.eval_forces(b, O.make_params(grid, flags=DEFAULT_FLAGS, npbc=(1, 1, 0), Rcut=10.0), golden["C"], pos=pos)
-    comp = np.zeros_like(Fo)
-    for fl in (DEFAULT_FLAGS & ~(GRID | NONBONDED), NONBONDED | PBC, GRID | PBC):
-        Fc, _ = O.eval_forces(b, O.make_params(grid, flags=fl, npbc=(1, 1, 0), Rcut=10.0), golden["C"], pos=pos)
-        comp += np.abs(Fc)
-    a, n, v = b.offsets()
-    for s in range(b.nsys):
-        sl = slice(v[s], v[s + 1])
-        ferr = np.abs(F[sl] - Fo[sl]).max() / comp[sl].max()
-        assert ferr < FTOL, (s, b.natoms[s], ferr)
-    eerr = np.abs(E - Eo).max(1) / np.maximum(np.abs(Eo[:, :3]).sum(1), 1e-9)
+    ferr, eerr = check_eval_components(world, b, grid_from_golden(golden), golden["C"], (1, 1, 0), 10.0)
+    assert ferr.max() < FTOL, ferr
     assert eerr.max() < ETOL, eerr
 
 
 def test_uneven_batch_vs_oracle(world, golden):
     sizes = [20, 33, 57, 64, 65, 120, 128, 129, 200, 256, 257, 400]
     b = S.make_systems(sizes, seed=3, topo_mode=1, sigma=0.1, cell=(11.28, 11.28, 40.0), npbc=(0, 0, 0))
-    ferr, eerr = check_eval(world, b, grid_from_golden(golden), golden["C"], DEFAULT_FLAGS, npbc=(0, 0, 0), Rcut=8.0)
+    ferr, eerr = check_eval_components(world, b, grid_from_golden(golden), golden["C"], (0, 0, 0), 8.0)
     assert ferr.max() < FTOL, ferr
     assert eerr.max() < ETOL, eerr
 
