@@ -184,10 +184,13 @@ def test_trained_proposal_gains_over_untrained(world, golden):
         acc = prop.warmstart(test.nsys, nsteps=2)
         _, E1 = world.eval()
         assert (E1[:, 3] <= E0[:, 3] + 1e-9 * np.abs(E0[:, 3])).all()
-        return float((E0[:, 3] - E1[:, 3]).sum()), int(acc.sum())
+        # per-atom energy drop, capped so that a few molecules with clashes
+        # (1e3..1e8 eV) do not decide the comparison
+        drop = np.minimum((E0[:, 3] - E1[:, 3]) / test.natoms, 1.0)
+        return float(drop.sum()), int(acc.sum())
 
     g_u, a_u = gain(False)
     g_t, a_t = gain(True)
-    print(f"energy lowered by warm start: untrained {g_u:.4f} eV ({a_u} moves kept), "
-          f"trained {g_t:.4f} eV ({a_t} moves kept)")
+    print(f"energy lowered by warm start (sum over systems of min(dE/atom, 1 eV)): untrained {g_u:.4f} "
+          f"({a_u} moves kept), trained {g_t:.4f} ({a_t} moves kept)")
     assert g_t > g_u, (g_t, g_u, a_t, a_u)
