@@ -25,7 +25,7 @@ namespace mmff {
 enum : int {
     F_BONDS = 1 << 0, F_PIPI = 1 << 1, F_PISIGMA = 1 << 2, F_ANGLES = 1 << 3,
     F_SUB_ANGLE_NB = 1 << 4, F_SUB_BOND_NB = 1 << 5, F_CLAMP_NB = 1 << 6,
-    F_NONBONDED = 1 << 7, F_GRID = 1 << 8, F_PBC = 1 << 9,
+    F_NONBONDED = 1 << 7, F_GRID = 1 << 8, F_PBC = 1 << 9, F_SURF = 1 << 10,
 };
 
 // status codes per system
@@ -50,7 +50,35 @@ struct Params {
     double Fconv2;
     int conv_mode;       // 0: sum f^2 ; 1: max |f|^2
     int nstep_max;       // steps allowed in this call
+    // Langevin drive (md_mode 1) instead of FIRE: MMFFsp3_loc::move_atom_Langevin
+    int md_mode;
+    float md_dt, md_gamma, md_noise;   // noise = sqrt(2 kB T gamma / dt)
+    unsigned long long md_seed;
+    int md_step0;                      // step index of the call's first step (random stream)
+    // direct substrate term (F_SURF): substrate atoms in world coordinates
+    const float4* __restrict__ surf_pos;
+    const float4* __restrict__ surf_REQ;   // (R0, sqrt(E0), Q sqrt(k_e), H)
+    int nsurf;
+    int snpbc[3];
+    float slv[9];                          // substrate lattice vectors a, b, c
+    float sK, sR2damp;                     // -alphaMorse, Rdamp^2
+    float sg0[3];                          // grid origin: world = local + gorg + sg0
 };
+
+// Counter-based uniform random number in [-1, 1) for the Langevin force:
+// SplitMix64 (Steele, Lea & Flood 2014) of (seed, vector, step, component);
+// 24 random bits, so the value is exact in float and double.
+__host__ __device__ inline unsigned long long mix64(unsigned long long z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+__host__ __device__ inline float langevin_rand(unsigned long long seed, long long vec, int step, int comp) {
+    const unsigned long long key =
+        seed ^ mix64(((unsigned long long)(unsigned)step << 32) ^ ((unsigned long long)vec << 2) ^ (unsigned long long)comp);
+    return (float)(mix64(key) >> 40) * (2.0f / 16777216.0f) - 1.0f;
+}
 
 struct Systems {
     int nsys;
@@ -149,6 +177,39 @@ __device__ __forceinline__ float pair_force(float dx, float dy, float dz, float4
         }
     }
     return F;
+}
+
+// Direct substrate term of one atom, getSurfMorse / getMorseQH
+// (relax_multi.cl:2741-2877, :166-181): Morse E0 e (e - 2), e = exp(K (r - R0)),
+// plus Coulomb k Q / sqrt(r^2 + Rdamp^2), over every substrate atom and its
+// images.  pw: atom position relative to the grid origin.  Returns (F, E).
+__device__ __forceinline__ float4 surf_atom(const Params& P, float3 pw, float4 Ri) {
+    const float K = P.sK, R2d = P.sR2damp;
+    pw = make_float3(pw.x + P.sg0[0], pw.y + P.sg0[1], pw.z + P.sg0[2]);
+    float fx = 0.f, fy = 0.f, fz = 0.f, E = 0.f;
+    for (int j = 0; j < P.nsurf; j++) {
+        const float4 sp = __ldg(P.surf_pos + j), Rj = __ldg(P.surf_REQ + j);
+        const float R0 = Ri.x + Rj.x, E0 = Ri.y * Rj.y, Q = Ri.z * Rj.z;
+        for (int iz = -P.snpbc[2]; iz <= P.snpbc[2]; iz++)
+            for (int iy = -P.snpbc[1]; iy <= P.snpbc[1]; iy++)
+                for (int ix = -P.snpbc[0]; ix <= P.snpbc[0]; ix++) {
+                    const float dx = pw.x - (sp.x + P.slv[0] * ix + P.slv[3] * iy + P.slv[6] * iz);
+                    const float dy = pw.y - (sp.y + P.slv[1] * ix + P.slv[4] * iy + P.slv[7] * iz);
+                    const float dz = pw.z - (sp.z + P.slv[2] * ix + P.slv[5] * iy + P.slv[8] * iz);
+                    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                    const float ir2d = 1.f / (r2 + R2d);
+                    const float ir = rsqrtf(r2);
+                    const float r = r2 * ir;
+                    const float e = expf(K * (r - R0));
+                    const float Ae = E0 * e;
+                    const float fM = Ae * 2.f * K * (e - 1.f);
+                    const float Eel = Q * sqrtf(ir2d);
+                    const float fr = fM * ir - Eel * ir2d;
+                    fx = fmaf(-dx, fr, fx); fy = fmaf(-dy, fr, fy); fz = fmaf(-dz, fr, fz);
+                    E += fmaf(Ae, e - 2.f, Eel);
+                }
+    }
+    return make_float4(fx, fy, fz, E);
 }
 
 // ----- bonded terms (one node atom), MMFFsp3_loc::eval_atom

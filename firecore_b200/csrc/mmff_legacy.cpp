@@ -187,6 +187,9 @@ struct LegacyWorld {
     bool bGrid = false;
     // FIRE (set_opt) -- pyBall/MMFF_multi.py:349 defaults
     double fire[9] = {0.1, 0.02, 0.2, 1.1, 0.5, 0.8, 5, 0.0, 10.0};
+    // thermal drive of init(T, gamma) (MolWorld_sp3_multi's TDrive): MDloop runs
+    // Langevin dynamics instead of FIRE when both are > 0
+    double T = 0.0, gamma = 0.0;
     // host mirrors (pyBall/MMFF_multi.py:238-256 shapes)
     std::vector<float> atoms, aforces, avel, constr, REQs, MMpars, BLs, BKs, Ksp, Kpp, lvecs, ilvecs, pbcshifts;
     std::vector<int> gneighs, gneighCell, gbkNeighs;
@@ -353,7 +356,8 @@ void* init(int nSys, char* xyz_name, char* surf_name, char* smile_name, bool bMM
            double gridStep, char* sElementTypes, char* sAtomTypes, char* sBondTypes, char* sAngleTypes, double T, double gamma,
            int nExplore, int nRelax, double pos_kick, double vel_kick, int GridFF) {
     (void)smile_name; (void)bMMFF; (void)bEpairs; (void)sElementTypes; (void)sAtomTypes; (void)sBondTypes; (void)sAngleTypes;
-    (void)T; (void)gamma; (void)nExplore; (void)nRelax; (void)pos_kick; (void)vel_kick;
+    (void)nExplore; (void)nRelax; (void)pos_kick; (void)vel_kick;
+    L.T = T; L.gamma = gamma;
     if (nSys < 1 || !xyz_name) { set_error("init: need nSys >= 1 and an xyz file"); return nullptr; }
     if (mmff_init_device(0)) { set_error(std::string("init: ") + mmff_last_error()); return nullptr; }
     XYZ X;
@@ -459,7 +463,22 @@ int run(int nstepMax, double dt, double Fconv, int ialg, double* outE, double* o
     return mx;
 }
 
-void MDloop(int perframe, double Ftol, int iParalel, int perVF) { (void)perVF; run(perframe, -1, Ftol > 0 ? Ftol : 1e-6, 0, nullptr, nullptr, iParalel); }
+// MolWorld_sp3_multi::MDloop: FIRE relaxation, or with init(T > 0, gamma > 0)
+// perframe steps of the Langevin drive (time step = the FIRE dt_max)
+void MDloop(int perframe, double Ftol, int iParalel, int perVF) {
+    (void)perVF;
+    if (L.ready && L.T > 0 && L.gamma > 0) {
+        static bool md_set = false;
+        if (!md_set && mmff_set_md(L.fire[0], L.gamma, L.T, 12345ull)) { set_error(mmff_last_error()); return; }
+        md_set = true;
+        if (mmff_md(perframe) || mmff_sync()) { set_error(mmff_last_error()); return; }
+        if (download_all(true, true)) return;
+        copy_sys_to_cpu(L.iSystemCur);
+        if (!L.trj_name.empty()) saveXYZ(L.trj_name.c_str(), "# MDloop", 1);
+        return;
+    }
+    run(perframe, -1, Ftol > 0 ? Ftol : 1e-6, 0, nullptr, nullptr, iParalel);
+}
 
 void set_opt(double dt_max, double dt_min, double damp_max, double finc, double fdec, double falpha, int minLastNeg,
              double cvf_min, double cvf_max) {

@@ -552,6 +552,18 @@ struct Engine {
         } else {
             for (int a = tid; a < natoms; a += T) fgr[a] = make_float4(0, 0, 0, 0);
         }
+        // --- direct substrate term (getSurfMorse), one thread per atom
+        if (flags & F_SURF) {
+            __syncthreads();
+            const float4* sR = at<float4>(L.REQ);
+            for (int a = tid; a < natoms; a += T) {
+                const float4 p = spos[a];
+                const float4 r = surf_atom(P, make_float3(p.x + gorg.x, p.y + gorg.y, p.z + gorg.z), sR[a]);
+                const float4 g = fgr[a];
+                fgr[a] = make_float4(g.x + r.x, g.y + r.y, g.z + r.z, 0.f);
+                if (ENERGY) Eg += (double)r.w;
+            }
+        }
     }
 
     // ------------------------------------------------------------------ phase 2
@@ -651,6 +663,36 @@ struct Engine {
         }
     }
 
+    // Langevin step (MMFFsp3_loc::move_atom_Langevin, MMFFsp3_loc.h:1191-1216):
+    // f - gamma v + uniform(-1,1) * sqrt(2 kB T gamma / dt), then v += f dt,
+    // p += v dt; pi vectors keep unit length and stay orthogonal to their force
+    __device__ void move_md(int step, float* mn, float* mx) {
+        float4* spos = at<float4>(L.pos);
+        float4* svel = at<float4>(L.vel);
+        const float4* fasm = at<float4>(L.fasm);
+        const float dt = P.md_dt, g = P.md_gamma, nz = P.md_noise;
+        for (int v = tid; v < nvecs; v += T) {
+            float3 f = f3(fasm[v]), ve = f3(svel[v]), p = f3(spos[v]);
+            const bool bPi = v >= natoms;
+            if (bPi) f = fma3(p, -dot3(p, f), f);
+            f = fma3(ve, -g, f);
+            const long long gv = (long long)voff + v;
+            f.x = fmaf(langevin_rand(P.md_seed, gv, step, 0), nz, f.x);
+            f.y = fmaf(langevin_rand(P.md_seed, gv, step, 1), nz, f.y);
+            f.z = fmaf(langevin_rand(P.md_seed, gv, step, 2), nz, f.z);
+            ve = fma3(f, dt, ve);
+            if (bPi) ve = fma3(p, -dot3(p, ve), ve);
+            p = fma3(ve, dt, p);
+            if (bPi) p = p * rsqrtf(dot3(p, p));
+            spos[v] = make_float4(p.x, p.y, p.z, 0.f);
+            svel[v] = make_float4(ve.x, ve.y, ve.z, 0.f);
+            if (!bPi) {
+                mn[0] = fminf(mn[0], p.x); mn[1] = fminf(mn[1], p.y); mn[2] = fminf(mn[2], p.z);
+                mx[0] = fmaxf(mx[0], p.x); mx[1] = fmaxf(mx[1], p.y); mx[2] = fmaxf(mx[2], p.z);
+            }
+        }
+    }
+
     __device__ void store_state(int status, int steps, float fconv, double dt, double damping, int lastNeg, double total) {
         const float4* spos = at<float4>(L.pos);
         const float4* svel = at<float4>(L.vel);
@@ -718,6 +760,14 @@ __global__ void __launch_bounds__(T, relax_min_blocks<T>()) relax_kernel(Params 
             E.assemble(vf, vv, ff, fmax2, bad);
             E.reduce4(vf, vv, ff, fmax2, bad);
             if (bad) { status = ST_NAN; break; }
+            if (P.md_mode) {        // Langevin drive: fixed number of steps, no FIRE
+                float mn[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, mx[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+                E.move_md(P.md_step0 + itr, mn, mx);
+                total += 1.0;
+                meas = sqrtf(fmax2);
+                E.bbox_reduce(mn, mx);
+                continue;
+            }
             // DynamicOpt::FIRE_update_params (FP64, identical in every thread)
             const double f_len = sqrt(ff), v_len = sqrt(vv);
             const double cos_vf = vf / (f_len * v_len + 1e-32);

@@ -500,6 +500,18 @@ struct WarpEngine {
                 }
             }
         }
+        if (flags & F_SURF) {           // direct substrate term (getSurfMorse)
+#pragma unroll
+            for (int k = 0; k < APL; k++) {
+                const int a = lane + 32 * k;
+                if (a < N) {
+                    const float4 p = sp[a];
+                    const float4 r = surf_atom(P, make_float3(p.x + lv[9], p.y + lv[10], p.z + lv[11]), sR[a]);
+                    if (k == 0) g0 = g0 + make_float3(r.x, r.y, r.z); else g1 = g1 + make_float3(r.x, r.y, r.z);
+                    if (ENERGY) Eg += (double)r.w;
+                }
+            }
+        }
         __syncwarp();   // recoil slots of every node written
         // ---- assembly (MMFFsp3_loc::assemble_atom)
 #pragma unroll
@@ -587,6 +599,37 @@ struct WarpEngine {
         __syncwarp();
     }
 
+    // Langevin step (MMFFsp3_loc::move_atom_Langevin, MMFFsp3_loc.h:1191-1216)
+    __device__ void move_md(int step) {
+        const float dt = P.md_dt, g = P.md_gamma, nz = P.md_noise;
+#pragma unroll
+        for (int k = 0; k < APL; k++) {
+            const int a = lane + 32 * k;
+#pragma unroll
+            for (int w = 0; w < 2; w++) {
+                const bool valid = (w == 0) ? (a < N) : (a < NN);
+                if (!valid) continue;
+                const int v = (w == 0) ? a : N + a;
+                float3 p = f3(sp[v]);
+                float3 f = (w == 0) ? fasm_a[k] : fasm_p[k];
+                float3 ve = (w == 0) ? va[k] : vp[k];
+                if (w == 1) f = fma3(p, -dot3(p, f), f);
+                f = fma3(ve, -g, f);
+                const long long gv = (long long)voff + v;
+                f.x = fmaf(langevin_rand(P.md_seed, gv, step, 0), nz, f.x);
+                f.y = fmaf(langevin_rand(P.md_seed, gv, step, 1), nz, f.y);
+                f.z = fmaf(langevin_rand(P.md_seed, gv, step, 2), nz, f.z);
+                ve = fma3(f, dt, ve);
+                if (w == 1) ve = fma3(p, -dot3(p, ve), ve);
+                p = fma3(ve, dt, p);
+                if (w == 1) p = p * rsqrtf(dot3(p, p));
+                sp[v] = make_float4(p.x, p.y, p.z, 0.f);
+                if (w == 0) va[k] = ve; else vp[k] = ve;
+            }
+        }
+        __syncwarp();
+    }
+
     __device__ void store(int status, int steps, float meas, double dt, double damping, int lastNeg, double total) {
         for (int v = lane; v < NV; v += 32) Y.pos[voff + v] = sp[v];
 #pragma unroll
@@ -637,6 +680,12 @@ __global__ void __launch_bounds__(128, MMFF_WARP_MINB) relax_warp_kernel(Params 
             bool bad;
             E.fire_sums(vf, vv, ff, fmax2, bad);
             if (bad) { status = ST_NAN; break; }
+            if (P.md_mode) {        // Langevin drive: fixed number of steps, no FIRE
+                E.move_md(P.md_step0 + itr);
+                total += 1.0;
+                meas = sqrtf(fmax2);
+                continue;
+            }
             // DynamicOpt::FIRE_update_params (DynamicOpt.cpp:250-267), FP64
             const double f_len = sqrt(ff), v_len = sqrt(vv);
             const double cos_vf = vf / (f_len * v_len + 1e-32);

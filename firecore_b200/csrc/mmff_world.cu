@@ -123,6 +123,15 @@ struct World {
     bool gkey_count = false;
     double gkey_fconv = 0.0;
     int version = 0;               // bumped by every change of parameters or systems
+    // direct substrate term
+    DBuf<float4> d_spos, d_sREQ;
+    int nsurf = 0, snpbc[3] = {1, 1, 0};
+    float slv[9] = {0};
+    double sRdamp = 1.0;
+    // Langevin drive
+    double md_dt = 0.05, md_gamma = 0.1, md_T = 300.0;
+    unsigned long long md_seed = 12345;
+    int md_step = 0;
 };
 
 World W;
@@ -163,6 +172,15 @@ Params make_params(bool for_eval, int nstep_max, double Fconv, int conv_mode) {
     P.Fconv2 = Fconv * Fconv;
     P.conv_mode = conv_mode;
     P.nstep_max = nstep_max;
+    if (W.nsurf > 0) {
+        P.surf_pos = W.d_spos.p; P.surf_REQ = W.d_sREQ.p; P.nsurf = W.nsurf;
+        for (int k = 0; k < 3; k++) { P.snpbc[k] = W.snpbc[k]; P.sg0[k] = (float)W.gpos0[k]; }
+        for (int k = 0; k < 9; k++) P.slv[k] = W.slv[k];
+        P.sK = (float)(-W.alphaMorse);
+        P.sR2damp = (float)(W.sRdamp * W.sRdamp);
+    } else {
+        P.flags &= ~F_SURF;
+    }
     return P;
 }
 
@@ -619,6 +637,57 @@ int mmff_relax(int nstep_max, double Fconv, int conv_mode) {
         W.gkey_count = W.count; W.gkey_version = W.version;
     }
     CK(cudaGraphLaunch(W.gexec, W.stream));
+    return 0;
+}
+
+// Substrate atoms for the direct term (flag F_SURF): positions [nsub][3] in
+// world coordinates, REQ [nsub][4] = (R0, sqrt(E0), Q, H), lattice vectors
+// [9] and image counts [3] of the substrate, Coulomb damping radius Rdamp.
+int mmff_surf_upload(int nsub, const double* spos, const double* sREQ, const double* lvec, const int* nPBC,
+                     double Rdamp) {
+    if (ensure_ready()) return -1;
+    if (nsub < 0 || (nsub > 0 && (!spos || !sREQ || !lvec || !nPBC))) return fail("mmff_surf_upload: bad arguments");
+    const double sqke = sqrt(14.3996448915);    // Coulomb constant [eV A / e^2], folded into the charges
+    std::vector<float4> hp(nsub), hr(nsub);
+    for (int i = 0; i < nsub; i++) {
+        hp[i] = make_float4((float)spos[3 * i], (float)spos[3 * i + 1], (float)spos[3 * i + 2], 0.f);
+        hr[i] = make_float4((float)sREQ[4 * i], (float)sREQ[4 * i + 1], (float)(sREQ[4 * i + 2] * sqke), (float)sREQ[4 * i + 3]);
+    }
+    if (upload(W.d_spos, hp) || upload(W.d_sREQ, hr)) return -1;
+    CK(cudaStreamSynchronize(W.stream));
+    W.nsurf = nsub;
+    for (int k = 0; k < 3; k++) W.snpbc[k] = nPBC ? nPBC[k] : 0;
+    for (int k = 0; k < 9; k++) W.slv[k] = lvec ? (float)lvec[k] : 0.f;
+    W.sRdamp = Rdamp;
+    W.version++;
+    return 0;
+}
+
+// Langevin drive parameters (MMFFsp3_loc::move_atom_Langevin): time step,
+// friction gamma, temperature T [K], random-stream seed (resets the step count).
+int mmff_set_md(double dt, double gamma, double T, unsigned long long seed) {
+    if (!(dt > 0) || gamma < 0 || T < 0) return fail("mmff_set_md: need dt > 0, gamma >= 0, T >= 0");
+    W.md_dt = dt; W.md_gamma = gamma; W.md_T = T; W.md_seed = seed; W.md_step = 0;
+    return 0;
+}
+
+// nsteps Langevin steps for every system (same persistent kernels as relax,
+// FIRE replaced by the drive; forces clamped by Flim when set).  Asynchronous.
+int mmff_md(int nsteps) {
+    if (ensure_ready()) return -1;
+    if (!W.nsys) return fail("no systems uploaded");
+    if (nsteps < 0) return fail("mmff_md: nsteps must be >= 0");
+    if (W.buckets_dirty && build_buckets()) return -1;
+    Params P = make_params(false, nsteps, -1.0, 1);
+    const double kB = 8.617333262e-5;     // eV/K (const_kB)
+    P.md_mode = 1;
+    P.md_dt = (float)W.md_dt;
+    P.md_gamma = (float)W.md_gamma;
+    P.md_noise = (float)sqrt(2.0 * kB * W.md_T * W.md_gamma / W.md_dt);
+    P.md_seed = W.md_seed;
+    P.md_step0 = W.md_step;
+    if (enqueue_relax(P)) return -1;
+    W.md_step += nsteps;
     return 0;
 }
 

@@ -19,7 +19,7 @@ from .systems import GridSpec, Substrate, SystemBatch
 # flag bits (include/MMFFmulti_lib.h, mmff_set_params)
 BONDS, PIPI, PISIGMA, ANGLES = 1, 2, 4, 8
 SUB_ANGLE_NB, SUB_BOND_NB, CLAMP_NB = 16, 32, 64
-NONBONDED, GRID, PBC = 128, 256, 512
+NONBONDED, GRID, PBC, SURF = 128, 256, 512, 1024
 # MolWorld_sp3::run_no_omp with bNonBondNeighs (ForceField.h:170-186)
 DEFAULT_FLAGS = BONDS | PIPI | PISIGMA | ANGLES | SUB_ANGLE_NB | NONBONDED | GRID | PBC
 
@@ -176,6 +176,23 @@ class World:
 
     def relax(self, nstep_max: int, Fconv: float = 1e-4, conv_mode: int = 1, sync: bool = True):
         _check(self.lib.mmff_relax(int(nstep_max), float(Fconv), int(conv_mode)), "mmff_relax")
+        if sync:
+            self.sync()
+
+    def surf_upload(self, sub: Substrate, Rdamp: float = 1.0):
+        """Substrate atoms for the direct term (flag SURF; no grid needed)."""
+        spos = np.ascontiguousarray(sub.spos, np.float64); sREQ = np.ascontiguousarray(sub.sREQ, np.float64)
+        lv = np.ascontiguousarray(sub.lvec.reshape(9), np.float64); nm = np.array(sub.nPBC_mors, np.int32)
+        _check(self.lib.mmff_surf_upload(spos.shape[0], _lib.ptr(spos), _lib.ptr(sREQ), _lib.ptr(lv), _lib.ptr(nm),
+                                         float(Rdamp)), "mmff_surf_upload")
+
+    def set_md(self, dt=0.05, gamma=0.1, T=300.0, seed=12345):
+        """Langevin drive parameters (resets the random stream's step count)."""
+        _check(self.lib.mmff_set_md(float(dt), float(gamma), float(T), int(seed)), "mmff_set_md")
+
+    def md(self, nsteps: int, sync: bool = True):
+        """nsteps Langevin steps of every system."""
+        _check(self.lib.mmff_md(int(nsteps)), "mmff_md")
         if sync:
             self.sync()
 

@@ -123,6 +123,22 @@ int mmff_relax(int nstep_max, double Fconv, int conv_mode);
  * Replaces the reference's host loop of kernel enqueues and round trips
  * every 10 steps (MolWorld_sp3_multi.h:843-908). */
 int mmff_set_graph(int on);
+/* Langevin drive ("explore" dynamics; replaces MMFFsp3_loc::move_atom_Langevin,
+ * MMFFsp3_loc.h:1191-1216, and the GPU drive of updateAtomsMMFFf4,
+ * relax_multi.cl:1163-1178): every step f <- f - gamma v + u * sqrt(2 kB T
+ * gamma / dt) with u uniform in [-1, 1) per component (counter-based stream
+ * of (seed, vector, step)), v += f dt, p += v dt; pi vectors stay unit and
+ * orthogonal.  mmff_set_md resets the step count of the random stream. */
+int mmff_set_md(double dt, double gamma, double T, unsigned long long seed);
+/* Direct substrate term (flag 1024 in mmff_set_params; replaces the kernel
+ * getSurfMorse with getMorseQH, relax_multi.cl:2741-2877, :166-181): per atom,
+ * Morse E0 e (e - 2), e = exp(-alphaMorse (r - R0)), plus Coulomb
+ * k Q / sqrt(r^2 + Rdamp^2), over the substrate atoms and their images.
+ * spos [nsub][3] world coordinates, sREQ [nsub][4] (R0, sqrt(E0), Q, H),
+ * lvec [9], nPBC [3].  Its energy adds to the grid energy slot. */
+int mmff_surf_upload(int nsub, const double* spos, const double* sREQ, const double* lvec, const int* nPBC,
+                     double Rdamp);
+int mmff_md(int nsteps);
 /* Autotuner (no counterpart in the reference, which uses one fixed work-group
  * size): for each size class present (0: <= 32 atoms, 1: <= 64, 3: <= 128,
  * 4: <= 256, 5: larger), time every candidate launch configuration (warp per

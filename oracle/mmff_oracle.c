@@ -613,6 +613,112 @@ void orc_relax(int nsys, const int* natoms, const int* nnode,
     free_offsets(o);
 }
 
+/* ---------------- direct substrate term (relax_multi.cl:2741-2877, :166-181) ---------------- */
+
+void orc_surf(int n, const double* pos, const double* REQ, int nsub, const double* spos,
+              const double* sREQ, const double* lvec, const int* nPBC, double alphaMorse,
+              double Rdamp, double* fe) {
+    const double kC = 14.3996448915, K = -alphaMorse, R2d = Rdamp * Rdamp;
+    for (int i = 0; i < n; i++) {
+        double F[3] = {0, 0, 0}, E = 0;
+        for (int j = 0; j < nsub; j++) {
+            const double R0 = REQ[4 * i] + sREQ[4 * j];
+            const double E0 = REQ[4 * i + 1] * sREQ[4 * j + 1];
+            const double Q = REQ[4 * i + 2] * sREQ[4 * j + 2];
+            for (int iz = -nPBC[2]; iz <= nPBC[2]; iz++)
+                for (int iy = -nPBC[1]; iy <= nPBC[1]; iy++)
+                    for (int ix = -nPBC[0]; ix <= nPBC[0]; ix++) {
+                        double d[3];
+                        for (int k = 0; k < 3; k++)
+                            d[k] = pos[3 * i + k] - (spos[3 * j + k] + lvec[k] * ix + lvec[3 + k] * iy + lvec[6 + k] * iz);
+                        const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+                        const double r = sqrt(r2);
+                        const double ir2d = 1.0 / (r2 + R2d);
+                        const double e = exp(K * (r - R0));
+                        const double Ae = E0 * e;
+                        const double fM = Ae * 2 * K * (e - 1);
+                        const double Eel = kC * Q * sqrt(ir2d);
+                        const double fr = fM / r - Eel * ir2d;
+                        for (int k = 0; k < 3; k++) F[k] -= d[k] * fr;
+                        E += Ae * (e - 2) + Eel;
+                    }
+        }
+        for (int k = 0; k < 3; k++) fe[4 * i + k] = F[k];
+        fe[4 * i + 3] = E;
+    }
+}
+
+/* ---------------- Langevin dynamics (MMFFsp3_loc.h:1191-1216) ---------------- */
+
+static unsigned long long orc_mix64(unsigned long long z) {   /* SplitMix64 finaliser */
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+double orc_langevin_rand(unsigned long long seed, long long vec, int step, int comp) {
+    const unsigned long long key = seed ^ orc_mix64(((unsigned long long)(unsigned)step << 32) ^
+                                                    ((unsigned long long)vec << 2) ^ (unsigned long long)comp);
+    return (double)(orc_mix64(key) >> 40) * (2.0 / 16777216.0) - 1.0;
+}
+
+void orc_md(int nsys, const int* natoms, const int* nnode, double* pos, double* vel,
+            const int* neighs, const int* neighCell, const int* bkneighs,
+            const double* REQs, const double* apars, const double* bLs,
+            const double* bKs, const double* Ksp, const double* Kpp,
+            const double* lvec, const double* gridC, const ORC_params* P,
+            int nsteps, double dt, double gamma, double T, unsigned long long seed, int step0,
+            double Flim, int nthreads) {
+    offsets_t o = make_offsets(nsys, natoms, nnode);
+    size_t nvtot = (size_t)o.voff[nsys];
+    double* force = (double*)calloc(nvtot * 3 + 3, sizeof(double));
+    const double kB = 8.617333262e-5;
+    const double noise = sqrt(2.0 * kB * T * gamma / dt);
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 1)
+#endif
+    for (int s = 0; s < nsys; s++) {
+        sysview S;
+        setup_view(&S, s, &o, natoms, nnode, pos, force, neighs, neighCell, bkneighs, REQs,
+                   apars, bLs, bKs, Ksp, Kpp, lvec, P);
+        double* p = pos + 3 * o.voff[s];
+        double* v = vel + 3 * o.voff[s];
+        double Ep[4] = {0, 0, 0, 0};
+        const int nv = S.nvecs;
+        for (int it = 0; it < nsteps; it++) {
+            eval_system(&S, P, gridC, Ep);
+            for (int i = 0; i < nv; i++) {
+                double* fi = S.force + 3 * i;
+                if (Flim > 0) {
+                    double fr2 = fi[0] * fi[0] + fi[1] * fi[1] + fi[2] * fi[2];
+                    if (fr2 > Flim * Flim) { double c = Flim / sqrt(fr2); fi[0] *= c; fi[1] *= c; fi[2] *= c; }
+                }
+                v3 f = ld3(fi), vi = ld3(v + 3 * i), pi = ld3(p + 3 * i);
+                const int bPi = i >= S.natoms;
+                if (bPi) f = vaddmul(f, pi, -vdot(pi, f));
+                f = vaddmul(f, vi, -gamma);
+                const long long gv = (long long)o.voff[s] + i;
+                v3 r = {orc_langevin_rand(seed, gv, step0 + it, 0), orc_langevin_rand(seed, gv, step0 + it, 1),
+                        orc_langevin_rand(seed, gv, step0 + it, 2)};
+                f = vaddmul(f, r, noise);
+                vi = vaddmul(vi, f, dt);
+                if (bPi) vi = vaddmul(vi, pi, -vdot(pi, vi));
+                pi = vaddmul(pi, vi, dt);
+                if (bPi) {
+                    double l = sqrt(pi.x * pi.x + pi.y * pi.y + pi.z * pi.z);
+                    pi = vmul(pi, 1.0 / l);
+                }
+                st3(p + 3 * i, pi); st3(v + 3 * i, vi);
+            }
+        }
+        free_view(&S);
+    }
+    free(force);
+    free_offsets(o);
+}
+
 /* ---------------- grid construction (GridFF.h:582-635, 847-891) ---------------- */
 
 void orc_grid_potentials(int nsub, const double* spos, const double* sREQ,

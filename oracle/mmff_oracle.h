@@ -97,6 +97,30 @@ void orc_relax(int nsys, const int* natoms, const int* nnode,
                int* nsteps_out, int* conv_out, double* Fout, double* Eout,
                int nthreads);
 
+/* Langevin dynamics, MMFFsp3_loc::move_atom_Langevin (MMFFsp3_loc.h:1191-1216):
+ * per step and vector f -= gamma v; f += u sqrt(2 kB T gamma / dt) with u in
+ * [-1,1) from orc_langevin_rand(seed, global vector index, step0 + step,
+ * component) (the reference draws randf(-1,1)); v += f dt; p += v dt; pi
+ * vectors: force and velocity projected, position renormalised.  Flim > 0
+ * clamps each force vector first (as in orc_relax). */
+void orc_md(int nsys, const int* natoms, const int* nnode, double* pos, double* vel,
+            const int* neighs, const int* neighCell, const int* bkneighs,
+            const double* REQs, const double* apars, const double* bLs,
+            const double* bKs, const double* Ksp, const double* Kpp,
+            const double* lvec, const double* gridC, const ORC_params* P,
+            int nsteps, double dt, double gamma, double T, unsigned long long seed, int step0,
+            double Flim, int nthreads);
+/* the uniform random numbers of orc_md (SplitMix64 of seed, vector, step, component) */
+double orc_langevin_rand(unsigned long long seed, long long vec, int step, int comp);
+
+/* Direct substrate term, getSurfMorse / getMorseQH (relax_multi.cl:2741-2877,
+ * :166-181), FP64: for n atoms at pos [n*3] with REQ [n*4] = (R0, sqrt E0,
+ * Q, H), against nsub substrate atoms and their images
+ * (-nPBC..nPBC along lvec rows): fe[i*4] = (F, E). */
+void orc_surf(int n, const double* pos, const double* REQ, int nsub, const double* spos,
+              const double* sREQ, const double* lvec, const int* nPBC, double alphaMorse,
+              double Rdamp, double* fe);
+
 /* B-spline GridFF sample of n points: fe[i*4] = (Fx,Fy,Fz,E) for PLQ[i*4]. */
 void orc_grid_sample(int n, const double* pos, const double* PLQ,
                      const double* gridC, const ORC_params* P, double* fe);

@@ -166,6 +166,41 @@ def relax(b, P: ORCParams, F: ORCFire, gridC=None, niter=1000, Fconv=1e-4, conv_
     return dict(pos=pos, vel=vel, fire_state=fire_state, nsteps=nsteps, converged=conv, F=Fout, E=Eout)
 
 
+def md(b, P: ORCParams, gridC=None, nsteps=10, dt=0.05, gamma=0.1, T=300.0, seed=12345, step0=0, pos=None,
+       vel=None, Flim=-1.0, nthreads=0):
+    """Langevin dynamics (MMFFsp3_loc::move_atom_Langevin) with the counter-based
+    noise stream of the device kernels. Returns dict(pos, vel)."""
+    lib = orc()
+    pos = np.array(b.pos if pos is None else pos, np.float64, order="C")
+    vel = np.zeros_like(pos) if vel is None else np.array(vel, np.float64, order="C")
+    keep = [np.ascontiguousarray(b.natoms, np.int32), np.ascontiguousarray(b.nnode, np.int32)]
+    g = None if gridC is None else np.ascontiguousarray(gridC, np.float64)
+    arrs = _sysarrays(b)
+    lib.orc_md(ctypes.c_int(b.nsys), _p(keep[0]), _p(keep[1]), _p(pos), _p(vel), *[_p(a) for a in arrs], _p(g),
+               ctypes.byref(P), ctypes.c_int(nsteps), ctypes.c_double(dt), ctypes.c_double(gamma), ctypes.c_double(T),
+               ctypes.c_ulonglong(seed), ctypes.c_int(step0), ctypes.c_double(Flim), ctypes.c_int(nthreads))
+    return dict(pos=pos, vel=vel)
+
+
+def surf(pos, REQ, sub, Rdamp=1.0):
+    """Direct substrate term of atoms at pos [n,3] with REQ [n,4]: [n,4] (F, E)."""
+    lib = orc()
+    pos = np.ascontiguousarray(pos, np.float64); REQ = np.ascontiguousarray(REQ, np.float64)
+    spos = np.ascontiguousarray(sub.spos, np.float64); sREQ = np.ascontiguousarray(sub.sREQ, np.float64)
+    lv = np.ascontiguousarray(sub.lvec.reshape(9), np.float64); nm = np.array(sub.nPBC_mors, np.int32)
+    fe = np.zeros((pos.shape[0], 4))
+    lib.orc_surf(ctypes.c_int(pos.shape[0]), _p(pos), _p(REQ), ctypes.c_int(spos.shape[0]), _p(spos), _p(sREQ),
+                 _p(lv), _p(nm), ctypes.c_double(sub.alphaMorse), ctypes.c_double(Rdamp), _p(fe))
+    return fe
+
+
+def langevin_rand(seed, vec, step, comp):
+    lib = orc()
+    lib.orc_langevin_rand.restype = ctypes.c_double
+    lib.orc_langevin_rand.argtypes = [ctypes.c_ulonglong, ctypes.c_longlong, ctypes.c_int, ctypes.c_int]
+    return lib.orc_langevin_rand(seed, vec, step, comp)
+
+
 def grid_sample(pos, PLQ, gridC, P: ORCParams):
     pos = np.ascontiguousarray(pos, np.float64); PLQ = np.ascontiguousarray(PLQ, np.float64)
     fe = np.zeros((pos.shape[0], 4))

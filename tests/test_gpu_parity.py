@@ -231,3 +231,53 @@ def test_bad_topology_rejected(world):
     b.neighs[3, 0] = 99                             # out of range
     with pytest.raises(RuntimeError, match="out of range"):
         world.upload(b)
+
+
+@pytest.mark.parametrize("sizes", [[24] * 8, [20, 57, 64, 65, 120, 200, 300]])
+def test_langevin_drive_vs_oracle(world, golden, sizes):
+    """Langevin drive (MMFFsp3_loc::move_atom_Langevin): 20 steps on the device
+    (warp- and CTA-per-system kernels) against the FP64 oracle fed the same
+    counter-based noise stream; the stream is reproducible and continues
+    across calls."""
+    grid = grid_from_golden(golden)
+    b = S.make_systems(sizes, seed=17, topo_mode=1, sigma=0.05, cell=(22.56, 22.56, 40.0))
+    world.set_params(flags=DEFAULT_FLAGS, npbc=(1, 1, 0), Rcut=10.0)
+    world.set_fire(FireParams(Flim=10.0))
+    world.upload(b)
+    pos0 = world.state()["pos"]
+    world.set_md(dt=0.05, gamma=0.5, T=300.0, seed=99)
+    world.md(10)
+    world.md(10)                          # continues the random stream at step 10
+    st = world.state()
+    r = O.md(b, O.make_params(grid, npbc=(1, 1, 0), Rcut=10.0), golden["C"], nsteps=20, dt=0.05, gamma=0.5,
+             T=300.0, seed=99, step0=0, pos=pos0, Flim=10.0)
+    assert np.abs(st["pos"] - pos0).max() > 1e-3
+    assert np.abs(st["pos"] - r["pos"]).max() < 1e-3, np.abs(st["pos"] - r["pos"]).max()
+    world.restore()
+    world.set_md(dt=0.05, gamma=0.5, T=300.0, seed=99)
+    world.md(20)
+    assert np.array_equal(world.state()["pos"], st["pos"])
+    world.set_fire(FireParams())
+
+
+def test_surface_direct_term_vs_oracle(world, golden):
+    """Direct substrate term (getSurfMorse / getMorseQH): Morse + damped
+    Coulomb of every atom against the substrate atoms and their images, warp-
+    and CTA-per-system kernels, against the FP64 oracle."""
+    from firecore_b200.world import SURF
+    sub = S.make_slab(ncell=2, layers=2)
+    b = S.make_systems([24] * 4 + [80, 150], seed=5, topo_mode=1, sigma=0.05, cell=(11.28, 11.28, 40.0))
+    world.surf_upload(sub, Rdamp=1.0)
+    world.set_params(flags=SURF, npbc=(0, 0, 0))
+    world.upload(b)
+    F, E = world.eval(True)
+    pos = world.state()["pos"]
+    a, n, v = b.offsets()
+    rows = np.concatenate([np.arange(v[s], v[s] + b.natoms[s]) for s in range(b.nsys)])
+    fe = O.surf(pos[rows], b.REQs, sub, 1.0)
+    err = np.abs(F[rows] - fe[:, :3]).max() / np.abs(fe[:, :3]).max()
+    assert err < 1e-5, err
+    Es = np.array([fe[a[s]:a[s + 1], 3].sum() for s in range(b.nsys)])
+    assert np.allclose(E[:, 2], Es, rtol=1e-5, atol=1e-5), (E[:, 2], Es)
+    world.lib.mmff_surf_upload(0, None, None, None, None, 1.0)
+    world.set_params(flags=DEFAULT_FLAGS)
