@@ -7,8 +7,9 @@
 // learned component; the network is this project's addition, checked against
 // the FP64 restatement in oracle/mlp_oracle.py.
 //
-// Network kernel: one CTA (128 threads, thread t = tile row t = TMEM lane t)
-// per SM, persistent over 128-atom tiles.  Per tile, all operands stay on chip:
+// Network kernel: one CTA of 256 threads per SM, persistent over 128-atom
+// tiles.  Warps w and w + 4 share TMEM lanes 32 (w % 4) .. + 31 (tile rows)
+// and split the columns of every epilogue in halves.  Per tile, all operands stay on chip:
 //   Z1 = X W1^T -> H1 = silu(Z1 + b1)                     (TMEM cols 0..127)
 //   Z2 = H1 W2^T -> H2 = silu(.), S2 = silu'(.)           (cols 128..255)
 //   Y  = H2 W3^T -> dY = 2 (Y + b3 - T) / B
@@ -157,22 +158,26 @@ struct NetArgs {
     float inv_batch, out_scale;
 };
 
+constexpr int NET_THREADS = 256;
+
 template <bool TRAIN>
-__global__ void __launch_bounds__(128, 1) mlp_kernel(NetArgs A) {
+__global__ void __launch_bounds__(NET_THREADS, 1) mlp_kernel(NetArgs A) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const uint32_t sb = smem_u32(sm);
     const int tid = threadIdx.x, warp = tid >> 5;
+    const int r = 32 * (warp & 3) + (tid & 31);   // tile row = TMEM lane of this thread
+    const int half = warp >> 2;                   // which half of the columns
     float* sbias = reinterpret_cast<float*>(sm + SM_BIAS);
     const uint32_t bar = sb + SM_MISC;
     uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + SM_MISC + 8);
 
     {   // weights, ones and biases into shared memory
         uint4* dst = reinterpret_cast<uint4*>(sm + SM_W1);
-        for (int i = tid; i < WP_BYTES / 16; i += 128) dst[i] = A.Wp[i];
+        for (int i = tid; i < WP_BYTES / 16; i += NET_THREADS) dst[i] = A.Wp[i];
         uint4* one = reinterpret_cast<uint4*>(sm + SM_ONE);
-        for (int i = tid; i < NOP * TILE * 2 / 16; i += 128) one[i] = make_uint4(0x3F803F80u, 0x3F803F80u, 0x3F803F80u, 0x3F803F80u);
-        for (int i = tid; i < HID; i += 128) { sbias[i] = A.prm[P_B1 + i]; sbias[HID + i] = A.prm[P_B2 + i]; }
+        for (int i = tid; i < NOP * TILE * 2 / 16; i += NET_THREADS) one[i] = make_uint4(0x3F803F80u, 0x3F803F80u, 0x3F803F80u, 0x3F803F80u);
+        for (int i = tid; i < HID; i += NET_THREADS) { sbias[i] = A.prm[P_B1 + i]; sbias[HID + i] = A.prm[P_B2 + i]; }
         if (tid < NOP) sbias[2 * HID + tid] = A.prm[P_B3 + tid];
     }
     if (tid == 0) mbar_init(bar, 1);
@@ -187,7 +192,8 @@ __global__ void __launch_bounds__(128, 1) mlp_kernel(NetArgs A) {
     __syncthreads();
     tc_after();
     const uint32_t tbase = *tslot;
-    const uint32_t trow = tbase + ((uint32_t)(32 * warp) << 16);   // this warp's 32 TMEM lanes
+    const uint32_t trow = tbase + ((uint32_t)(32 * (warp & 3)) << 16);   // this warp's 32 TMEM lanes
+    const int c0 = half * (HID / 2), c1 = c0 + HID / 2;                   // this thread's epilogue columns
 
     uint32_t phase = 0;
     bool failed = false;
@@ -214,44 +220,47 @@ __global__ void __launch_bounds__(128, 1) mlp_kernel(NetArgs A) {
     float v[16], w[16];
     for (int tile = blockIdx.x; tile < A.ntile; tile += gridDim.x) {
         const bool acc = done > 0;
-        const int row = tile * TILE + tid;
+        const int row = tile * TILE + r;
         {
             const uint4* src = A.X + (size_t)tile * (TILE * K0 * 2 / 16);
             uint4* dst = reinterpret_cast<uint4*>(sm + SM_X);
-            for (int i = tid; i < TILE * K0 * 2 / 16; i += 128) dst[i] = src[i];
+            for (int i = tid; i < TILE * K0 * 2 / 16; i += NET_THREADS) dst[i] = src[i];
         }
         sync_for_mma();
         if (tid == 0) issue(sb, tbase, OP_L1, false);
         if (!complete()) { failed = true; break; }
-        for (int c = 0; c < HID; c += 16) {          // H1 = silu(Z1 + b1)
+        for (int c = c0; c < c1; c += 16) {          // H1 = silu(Z1 + b1)
             tm_ld16(trow + TM_Z1 + c, v);
 #pragma unroll
             for (int j = 0; j < 16; j++) v[j] = silu_f(v[j] + sbias[c + j]);
-            st_row16(sm + SM_H1, tid, c, HID, v);
+            st_row16(sm + SM_H1, r, c, HID, v);
         }
         sync_for_mma();
         if (tid == 0) issue(sb, tbase, OP_L2, false);
         if (!complete()) { failed = true; break; }
-        for (int c = 0; c < HID; c += 16) {          // H2 = silu(Z2 + b2), S2 = silu'(Z2 + b2)
+        for (int c = c0; c < c1; c += 16) {          // H2 = silu(Z2 + b2), S2 = silu'(Z2 + b2)
             tm_ld16(trow + TM_WORK + c, v);
 #pragma unroll
             for (int j = 0; j < 16; j++) { const float z = v[j] + sbias[HID + c + j]; v[j] = silu_f(z); w[j] = dsilu_f(z); }
-            st_row16(sm + SM_H2, tid, c, HID, v);
-            if (TRAIN) st_row16(sm + SM_S2, tid, c, HID, w);
+            st_row16(sm + SM_H2, r, c, HID, v);
+            if (TRAIN) st_row16(sm + SM_S2, r, c, HID, w);
         }
         sync_for_mma();
         if (tid == 0) issue(sb, tbase, OP_L3, false);
         if (!complete()) { failed = true; break; }
-        tm_ld16(trow + TM_WORK, v);
+        if (half == 0) {
+            tm_ld16(trow + TM_WORK, v);
 #pragma unroll
-        for (int j = 0; j < NOP; j++) v[j] += sbias[2 * HID + j];
+            for (int j = 0; j < NOP; j++) v[j] += sbias[2 * HID + j];
+        }
         if (!TRAIN) {
-            if (row < A.nrows) A.out[row] = make_float4(v[0] * A.out_scale, v[1] * A.out_scale, v[2] * A.out_scale, 0.f);
+            if (half == 0 && row < A.nrows)
+                A.out[row] = make_float4(v[0] * A.out_scale, v[1] * A.out_scale, v[2] * A.out_scale, 0.f);
             done++;
             sync_for_mma();      // TMEM reads of this tile finish before the next tile's products
             continue;
         }
-        {   // loss and dY = 2 (y - t) w / B (padding rows have w = 0)
+        if (half == 0) {   // loss and dY = 2 (y - t) w / B (padding rows have w = 0)
             const float4 t = A.T[row];
             const float d0 = (v[0] - t.x) * t.w, d1 = (v[1] - t.y) * t.w, d2 = (v[2] - t.z) * t.w;
             lsum += d0 * d0 + d1 * d1 + d2 * d2;
@@ -260,27 +269,27 @@ __global__ void __launch_bounds__(128, 1) mlp_kernel(NetArgs A) {
             for (int j = 0; j < 16; j++) w[j] = 0.f;
             w[0] = bf_round(s * d0); w[1] = bf_round(s * d1); w[2] = bf_round(s * d2);
             db3[0] += w[0]; db3[1] += w[1]; db3[2] += w[2];
-            st_row16(sm + SM_DY, tid, 0, NOP, w);
+            st_row16(sm + SM_DY, r, 0, NOP, w);
         }
         sync_for_mma();
         if (tid == 0) { issue(sb, tbase, OP_DW3, acc); issue(sb, tbase, OP_DH2, false); }
         if (!complete()) { failed = true; break; }
-        for (int c = 0; c < HID; c += 16) {          // dZ2 = dH2 * S2 (in place of S2)
+        for (int c = c0; c < c1; c += 16) {          // dZ2 = dH2 * S2 (in place of S2)
             tm_ld16(trow + TM_WORK + c, v);
-            ld_row16(sm + SM_S2, tid, c, HID, w);
+            ld_row16(sm + SM_S2, r, c, HID, w);
 #pragma unroll
             for (int j = 0; j < 16; j++) v[j] *= w[j];
-            st_row16(sm + SM_S2, tid, c, HID, v);
+            st_row16(sm + SM_S2, r, c, HID, v);
         }
         sync_for_mma();
         if (tid == 0) { issue(sb, tbase, OP_DW2, acc); issue(sb, tbase, OP_DB2, acc); issue(sb, tbase, OP_DH1, false); }
         if (!complete()) { failed = true; break; }
-        for (int c = 0; c < HID; c += 16) {          // dZ1 = dH1 * silu'(Z1 + b1), into the H2 buffer
+        for (int c = c0; c < c1; c += 16) {          // dZ1 = dH1 * silu'(Z1 + b1), into the H2 buffer
             tm_ld16(trow + TM_WORK + c, v);
             tm_ld16(trow + TM_Z1 + c, w);
 #pragma unroll
             for (int j = 0; j < 16; j++) v[j] *= bf_round(dsilu_f(w[j] + sbias[c + j]));
-            st_row16(sm + SM_H2, tid, c, HID, v);
+            st_row16(sm + SM_H2, r, c, HID, v);
         }
         sync_for_mma();
         if (tid == 0) { issue(sb, tbase, OP_DW1, acc); issue(sb, tbase, OP_DB1, acc); }
@@ -292,27 +301,30 @@ __global__ void __launch_bounds__(128, 1) mlp_kernel(NetArgs A) {
         // this CTA's gradient sums, plain stores into its own slice (reduced
         // over CTAs by reduce_grad_kernel: no atomics, deterministic order)
         float* g = A.gpart + (size_t)blockIdx.x * P_TOTAL;
-        float* red = reinterpret_cast<float*>(sm + SM_X);      // X tile no longer needed: 4 warps x 4 floats
+        float* red = reinterpret_cast<float*>(sm + SM_X);      // X tile no longer needed: 8 warps x 4 floats
         if (!failed && done > 0) {
-            for (int c = 0; c < HID; c += 16) {
+            for (int c = c0; c < c1; c += 16) {
                 tm_ld16(trow + TM_DW2 + c, v);
 #pragma unroll
-                for (int j = 0; j < 16; j++) g[P_W2 + tid * HID + c + j] = v[j];
+                for (int j = 0; j < 16; j++) g[P_W2 + r * HID + c + j] = v[j];
             }
-            for (int c = 0; c < K0; c += 16) {
+            // dW1: 5 chunks of 16 columns, 3 in the first half, 2 in the second
+            for (int c = half ? 48 : 0; c < (half ? K0 : 48); c += 16) {
                 tm_ld16(trow + TM_DW1 + c, v);
 #pragma unroll
-                for (int j = 0; j < 16; j++) g[P_W1 + tid * K0 + c + j] = v[j];
+                for (int j = 0; j < 16; j++) g[P_W1 + r * K0 + c + j] = v[j];
             }
-            tm_ld16(trow + TM_DW3, v);
+            if (half == 0) {
+                tm_ld16(trow + TM_DW3, v);
 #pragma unroll
-            for (int j = 0; j < NOP; j++) g[P_W3 + j * HID + tid] = v[j];
-            tm_ld16(trow + TM_DB1, v);
-            g[P_B1 + tid] = v[0];
-            tm_ld16(trow + TM_DB2, v);
-            g[P_B2 + tid] = v[0];
+                for (int j = 0; j < NOP; j++) g[P_W3 + j * HID + r] = v[j];
+                tm_ld16(trow + TM_DB1, v);
+                g[P_B1 + r] = v[0];
+                tm_ld16(trow + TM_DB2, v);
+                g[P_B2 + r] = v[0];
+            }
         } else {
-            for (int i = tid; i < P_B3; i += 128) g[i] = 0.f;
+            for (int i = tid; i < P_B3; i += NET_THREADS) g[i] = 0.f;
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -329,12 +341,12 @@ __global__ void __launch_bounds__(128, 1) mlp_kernel(NetArgs A) {
         __syncthreads();
         if (tid < NOP) {
             float b = 0.f;
-            if (tid < NOUT) for (int q = 0; q < 4; q++) b += red[4 * q + 1 + tid];
+            if (tid < NOUT) for (int q = 0; q < NET_THREADS / 32; q++) b += red[4 * q + 1 + tid];
             g[P_B3 + tid] = b;
         }
         if (tid == 0) {
             double l = 0.0;
-            for (int q = 0; q < 4; q++) l += (double)red[4 * q];
+            for (int q = 0; q < NET_THREADS / 32; q++) l += (double)red[4 * q];
             A.lpart[blockIdx.x] = l * (double)A.inv_batch;
         }
     }
@@ -628,10 +640,10 @@ int run_net(bool train, const uint8_t* X, const float4* T, int ntile, int nrows,
     a.prm = N.prm.p; a.gpart = N.gpart.p; a.lpart = N.lpart.p; a.out = out; a.err = N.err.p;
     a.ntile = ntile; a.nrows = nrows; a.inv_batch = inv_batch; a.out_scale = N.out_scale;
     if (train) {
-        mlp_kernel<true><<<grid, 128, SM_ALLOC, st>>>(a);
+        mlp_kernel<true><<<grid, NET_THREADS, SM_ALLOC, st>>>(a);
         reduce_grad_kernel<<<(P_TOTAL + 255) / 256, 256, 0, st>>>(N.gpart.p, N.lpart.p, grid, N.grad.p, N.loss.p);
     } else {
-        mlp_kernel<false><<<grid, 128, SM_ALLOC, st>>>(a);
+        mlp_kernel<false><<<grid, NET_THREADS, SM_ALLOC, st>>>(a);
     }
     MCK(cudaGetLastError());
     return 0;
