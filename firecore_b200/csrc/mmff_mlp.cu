@@ -144,6 +144,8 @@ constexpr int P_W1 = 0, P_B1 = P_W1 + HID * K0, P_W2 = P_B1 + HID, P_B2 = P_W2 +
 // packed bf16 weight image: W1 | W2 | W3, laid out exactly as in shared memory
 constexpr int WP_W1 = 0, WP_W2 = HID * K0 * 2, WP_W3 = WP_W2 + HID * HID * 2, WP_BYTES = WP_W3 + NOP * HID * 2;
 static_assert(SM_W2 - SM_W1 == WP_W2 && SM_W3 - SM_W1 == WP_W3, "weight image must match the smem map");
+static_assert(P_W1 % 4 == 0 && P_W2 % 4 == 0 && K0 % 4 == 0 && HID % 4 == 0 && P_TOTAL % 4 == 0,
+              "16-byte gradient stores need 16-byte aligned rows");
 
 struct NetArgs {
     const uint4* X;          // packed input tiles [ntile][128 x 80 bf16]
@@ -303,16 +305,19 @@ __global__ void __launch_bounds__(NET_THREADS, 1) mlp_kernel(NetArgs A) {
         float* g = A.gpart + (size_t)blockIdx.x * P_TOTAL;
         float* red = reinterpret_cast<float*>(sm + SM_X);      // X tile no longer needed: 8 warps x 4 floats
         if (!failed && done > 0) {
+            // 16-byte stores (every row start and chunk is 64-byte aligned)
             for (int c = c0; c < c1; c += 16) {
                 tm_ld16(trow + TM_DW2 + c, v);
+                float4* d = reinterpret_cast<float4*>(g + P_W2 + r * HID + c);
 #pragma unroll
-                for (int j = 0; j < 16; j++) g[P_W2 + r * HID + c + j] = v[j];
+                for (int j = 0; j < 4; j++) d[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
             }
             // dW1: 5 chunks of 16 columns, 3 in the first half, 2 in the second
             for (int c = half ? 48 : 0; c < (half ? K0 : 48); c += 16) {
                 tm_ld16(trow + TM_DW1 + c, v);
+                float4* d = reinterpret_cast<float4*>(g + P_W1 + r * K0 + c);
 #pragma unroll
-                for (int j = 0; j < 16; j++) g[P_W1 + r * K0 + c + j] = v[j];
+                for (int j = 0; j < 4; j++) d[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
             }
             if (half == 0) {
                 tm_ld16(trow + TM_DW3, v);

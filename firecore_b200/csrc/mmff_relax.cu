@@ -422,7 +422,14 @@ struct Engine {
             const bool pbc = (flags & F_PBC) != 0;
             const int npx = pbc ? P.npbc[0] : 0, npy = pbc ? P.npbc[1] : 0, npz = pbc ? P.npbc[2] : 0;
             const int nxi = 2 * npx + 1, nyi = 2 * npy + 1;
-            const bool lists = L.nimg > 0;          // cutoff + PBC: candidate lists per shifted image
+            // cutoff + PBC: candidate lists per shifted image, built only when the
+            // bounding-box test keeps some shifted image (block-uniform)
+            bool any_shift = false;
+            for (int iz = -npz; iz <= npz; iz++)
+                for (int iy = -npy; iy <= npy; iy++)
+                    for (int ix = -npx; ix <= npx; ix++)
+                        if ((ix | iy | iz) != 0) any_shift |= image_active(ix, iy, iz);
+            const bool lists = L.nimg > 0 && any_shift;
             if (lists) build_candidates();
             const int central = (npz * nyi + npy) * nxi + npx;
             const unsigned short* clist = at<unsigned short>(L.clist);
@@ -443,7 +450,7 @@ struct Engine {
                                      (float)facc[3 * a + 2] * (1.f / kFix), 0.f);
             // without candidate lists: the other images of the bounding-box test,
             // ordered pairs (i, j + shift), S lanes per atom
-            if (!lists && (npx | npy | npz)) {
+            if (!lists && any_shift) {
                 __syncthreads();
                 const int nunits = natoms * S;
                 for (int u0 = 0; u0 < nunits; u0 += T) {
