@@ -389,6 +389,55 @@ struct Engine {
         }
     }
 
+    // GridFF B-spline of every atom, 4 lanes per atom (x-slices), by the
+    // threads t0 = 0 .. nt-1 of the caller (whole warps); zero without a grid
+    __device__ void grid_phase(int t0, int nt, float4* fgr, double& Eg) {
+        const float4* spos = at<float4>(L.pos);
+        if (!(P.flags & F_GRID)) {
+            for (int a = t0; a < natoms; a += nt) fgr[a] = make_float4(0, 0, 0, 0);
+            return;
+        }
+        const float4* sPLQ = at<float4>(L.PLQ);
+        const int nunits = natoms * 4;
+        for (int u0 = 0; u0 < nunits; u0 += nt) {
+            const int u = u0 + t0;
+            const int i = u >> 2, a = u & 3;
+            float4 r = make_float4(0, 0, 0, 0);
+            if (i < natoms) {
+                const float4 p = spos[i];
+                const float3 uu = make_float3((p.x + gorg.x) * P.ginv[0], (p.y + gorg.y) * P.ginv[1],
+                                              (p.z + gorg.z) * P.ginv[2]);
+                r = grid_slice(P.grid, P.gn[0], P.gn[1], P.gn[2], uu, sPLQ[i], a);
+            }
+#pragma unroll
+            for (int o = 2; o > 0; o >>= 1) {
+                r.x += __shfl_xor_sync(0xffffffffu, r.x, o);
+                r.y += __shfl_xor_sync(0xffffffffu, r.y, o);
+                r.z += __shfl_xor_sync(0xffffffffu, r.z, o);
+                r.w += __shfl_xor_sync(0xffffffffu, r.w, o);
+            }
+            if (i < natoms && a == 0) {
+                fgr[i] = make_float4(r.x * P.gmi[0], r.y * P.gmi[1], r.z * P.gmi[2], 0.f);
+                if (ENERGY) Eg += (double)r.w;
+            }
+        }
+    }
+
+    // Threads given to the bonded terms when the GridFF runs beside them on
+    // the remaining warps; T = no split.  Cost model in units of one grid
+    // round (4 lanes x 16 float4 gathers per atom): one bonded pass (one node
+    // per thread) costs ~10 rounds.  Split when the longer of the two
+    // concurrent parts beats running them one after the other.
+    __device__ __forceinline__ int bonded_grid_split() const {
+        if (!(P.flags & F_GRID)) return T;
+        const int Tb = ((nnode + 31) / 32) * 32;
+        if (Tb >= T || Tb == 0) return T;
+        const int Tg = T - Tb;
+        const int now = 10 * ((nnode + T - 1) / T) + (4 * natoms + T - 1) / T;
+        const int par = max(10, (4 * natoms + Tg - 1) / Tg);
+        return par < now ? Tb : T;
+    }
+
     // ------------------------------------------------------------------ phase 1
     // returns this thread's energy contributions (only meaningful if ENERGY)
     __device__ void forces(double& Eb, double& Enb, double& Eg) {
@@ -401,8 +450,17 @@ struct Engine {
         const int4* sng = at<int4>(L.ng);
         const int4* sngC = at<int4>(L.ngC);
         float4* fng = at<float4>(L.fng);
+        // Bonded terms and the GridFF stencil are independent: when the nodes
+        // fill only part of the block, the other warps sample the grid at the
+        // same time (block-uniform choice, see bonded_grid_split)
+        const int Tb = bonded_grid_split();
+        const bool split = Tb < T;
+        if (split && tid >= Tb) {
+            grid_phase(tid - Tb, T - Tb, fgr, Eg);
+        }
         // --- bonded (nodes); caps get a zero own-force
-        for (int ia = tid; ia < natoms; ia += T) {
+        if (tid < Tb)
+        for (int ia = tid; ia < natoms; ia += Tb) {
             if (ia >= nnode) { fasm[ia] = make_float4(0, 0, 0, 0); continue; }
             BondedOut o;
             eval_atom<ENERGY>(ia, natoms, nnode, flags, P.Fmax2NB, spos, sREQ, sng[ia], sngC[ia],
@@ -530,35 +588,8 @@ struct Engine {
         } else {
             for (int a = tid; a < natoms; a += T) fnb[a] = make_float4(0, 0, 0, 0);
         }
-        // --- GridFF B-spline: 4 lanes per atom (x-slices)
-        if (flags & F_GRID) {
-            const float4* sPLQ = at<float4>(L.PLQ);
-            const int nunits = natoms * 4;
-            for (int u0 = 0; u0 < nunits; u0 += T) {
-                const int u = u0 + tid;
-                const int i = u >> 2, a = u & 3;
-                float4 r = make_float4(0, 0, 0, 0);
-                if (i < natoms) {
-                    const float4 p = spos[i];
-                    const float3 uu = make_float3((p.x + gorg.x) * P.ginv[0], (p.y + gorg.y) * P.ginv[1],
-                                                  (p.z + gorg.z) * P.ginv[2]);
-                    r = grid_slice(P.grid, P.gn[0], P.gn[1], P.gn[2], uu, sPLQ[i], a);
-                }
-#pragma unroll
-                for (int o = 2; o > 0; o >>= 1) {
-                    r.x += __shfl_xor_sync(0xffffffffu, r.x, o);
-                    r.y += __shfl_xor_sync(0xffffffffu, r.y, o);
-                    r.z += __shfl_xor_sync(0xffffffffu, r.z, o);
-                    r.w += __shfl_xor_sync(0xffffffffu, r.w, o);
-                }
-                if (i < natoms && a == 0) {
-                    fgr[i] = make_float4(r.x * P.gmi[0], r.y * P.gmi[1], r.z * P.gmi[2], 0.f);
-                    if (ENERGY) Eg += (double)r.w;
-                }
-            }
-        } else {
-            for (int a = tid; a < natoms; a += T) fgr[a] = make_float4(0, 0, 0, 0);
-        }
+        // --- GridFF B-spline (unless it ran beside the bonded terms)
+        if (!split) grid_phase(tid, T, fgr, Eg);
         // --- direct substrate term (getSurfMorse), one thread per atom
         if (flags & F_SURF) {
             __syncthreads();
