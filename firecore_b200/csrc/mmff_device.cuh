@@ -459,8 +459,7 @@ struct SmemLayout {
     // offsets in bytes
     int pos, vel, fasm, fnb, fgrid, REQ, PLQ, ng, ngC, bk, apar, bL, bK, ksp, kpp, fng, red;
     int cwords, cpref, ccnt, clist;     // per-image candidate lists (cutoff + PBC only)
-    int facc;                           // fixed-point force sums of the central image [3 * maxNA] int64
-    int bblk, total;                    // bounding box per 32-atom block (6 floats)
+    int facc, total;                    // fixed-point force sums of the central image [3 * maxNA] int64
 };
 
 // number of shifted (non-central) PBC images of the pair term
@@ -498,7 +497,6 @@ __host__ __device__ inline SmemLayout smem_layout(int maxNA, int maxNN, int T, i
     L.ccnt = take(4 * nimg);                // candidates per image
     L.clist = take(2 * nimg * maxNA);       // candidate atom indices per image, ascending
     L.facc = take(8 * 3 * maxNA);
-    L.bblk = take(4 * 6 * L.nwords);
     L.total = o;
     return L;
 }

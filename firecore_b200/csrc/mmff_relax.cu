@@ -380,18 +380,7 @@ struct Engine {
             if (u < noff) {
                 int bi = 0, rem = u;
                 while (rem >= B - 1 - bi) { rem -= B - 1 - bi; bi++; }
-                const int bj = bi + 1 + rem;
-                if (P.Rc2 > 0.f) {          // blocks whose boxes are beyond the cutoff: nothing to do
-                    const float* bb = at<float>(L.bblk);
-                    float g2 = 0.f;
-#pragma unroll
-                    for (int k = 0; k < 3; k++) {
-                        const float g = fmaxf(0.f, fmaxf(bb[6 * bj + k] - bb[6 * bi + 3 + k], bb[6 * bi + k] - bb[6 * bj + 3 + k]));
-                        g2 = fmaf(g, g, g2);
-                    }
-                    if (g2 >= P.Rc2) continue;
-                }
-                off_tile<HB>(bi, bj, spos, sREQ, pbc, central, facc, ec);
+                off_tile<HB>(bi, bi + 1 + rem, spos, sREQ, pbc, central, facc, ec);
             } else {
                 const int d = 2 * (u - noff);
                 diag_tile<HB>(d, spos, sREQ, pbc, central, facc, ec);
@@ -506,19 +495,6 @@ struct Engine {
             // central image: every unordered pair once, into fixed-point sums
             long long* facc = at<long long>(L.facc);
             for (int a = tid; a < 3 * natoms; a += T) facc[a] = 0;
-            if (P.Rc2 > 0.f) {              // bounding box of every 32-atom block (one warp each)
-                float* bb = at<float>(L.bblk);
-                for (int blk = warp; blk < (natoms + 31) / 32; blk += L.nwarps) {
-                    const int i = blk * 32 + lane;
-                    const float4 p = spos[min(i, natoms - 1)];
-                    const float mn[3] = {wmin(p.x), wmin(p.y), wmin(p.z)};
-                    const float mx[3] = {wmax(p.x), wmax(p.y), wmax(p.z)};
-                    if (lane == 0) {
-#pragma unroll
-                        for (int k = 0; k < 3; k++) { bb[6 * blk + k] = mn[k]; bb[6 * blk + 3 + k] = mx[k]; }
-                    }
-                }
-            }
             __syncthreads();
             {
                 float ec = 0.f;
