@@ -304,6 +304,21 @@ struct Engine {
         return t;
     }
 
+    // excluded j-slots of block bj for this lane's atom: all if the atom is a
+    // padding slot, padding slots of bj, and the atom's bonded neighbours in bj
+    __device__ __forceinline__ uint32_t tile_mask(const TileAtom& a, int bj) const {
+        if (!a.v) return ~0u;
+        const int nvalid = natoms - 32 * bj;
+        uint32_t m = nvalid >= 32 ? 0u : ~((1u << nvalid) - 1u);
+        const int e[4] = {a.e1, a.e2, a.e3, a.e4};
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int d = e[k] - 32 * bj;
+            if (e[k] >= 0 && d >= 0 && d < 32) m |= 1u << d;
+        }
+        return m;
+    }
+
     template <bool HB>
     __device__ void off_tile(int bi, int bj, const float4* spos, const float4* sREQ, bool pbc, int central,
                              long long* facc, float& ec) {
@@ -312,15 +327,17 @@ struct Engine {
         const float rc = CUT ? sqrtf(1.f / kq) : 0.f;
         const int i = bi * 32 + lane;
         const TileAtom a = tile_atom(i, spos, sREQ, pbc, central);
+        const uint32_t xm = tile_mask(a, bj);
         float3 fi = make_float3(0.f, 0.f, 0.f), rj = make_float3(0.f, 0.f, 0.f);
         bool ok;
         float e = 0.f;
 #pragma unroll kTileUnroll
         for (int s = 0; s < 32; s++) {
-            const int j = bj * 32 + ((lane + s) & 31);
-            const bool vj = j < natoms;
-            const float4 pj = spos[vj ? j : 0], Rj = sREQ[vj ? j : 0];
-            const bool excl = !a.v || !vj || j == a.e1 || j == a.e2 || j == a.e3 || j == a.e4;
+            const int jl = (lane + s) & 31;
+            const int j = bj * 32 + jl;
+            const int jc = min(j, natoms - 1);
+            const float4 pj = spos[jc], Rj = sREQ[jc];
+            const bool excl = (xm >> jl) & 1u;
             const float dx = pj.x - a.p.x, dy = pj.y - a.p.y, dz = pj.z - a.p.z;
             const float F = pair_force<ENERGY, HB>(dx, dy, dz, a.R, Rj, excl, Rc2, kq, rc, CUT, ok, e);
             fi.x = fmaf(dx, F, fi.x); fi.y = fmaf(dy, F, fi.y); fi.z = fmaf(dz, F, fi.z);
@@ -345,16 +362,16 @@ struct Engine {
         const float rc = CUT ? sqrtf(1.f / kq) : 0.f;
         const int i = b * 32 + lane;
         const TileAtom a = tile_atom(i, spos, sREQ, pbc, central);
+        const uint32_t xm = tile_mask(a, b);
         float3 fi = make_float3(0.f, 0.f, 0.f);
         bool ok;
         float e = 0.f;
 #pragma unroll kTileUnroll
         for (int s = 1; s <= 16; s++) {
-            const int j = b * 32 + ((lane + s) & 31);
-            const bool vj = j < natoms;
-            const float4 pj = spos[vj ? j : 0], Rj = sREQ[vj ? j : 0];
-            const bool half = (s < 16) || (lane < 16);
-            const bool excl = !a.v || !vj || !half || j == a.e1 || j == a.e2 || j == a.e3 || j == a.e4;
+            const int jl = (lane + s) & 31;
+            const int jc = min(b * 32 + jl, natoms - 1);
+            const float4 pj = spos[jc], Rj = sREQ[jc];
+            const bool excl = ((xm >> jl) & 1u) || (s == 16 && lane >= 16);
             const float dx = pj.x - a.p.x, dy = pj.y - a.p.y, dz = pj.z - a.p.z;
             const float F = pair_force<ENERGY, HB>(dx, dy, dz, a.R, Rj, excl, Rc2, kq, rc, CUT, ok, e);
             fi.x = fmaf(dx, F, fi.x); fi.y = fmaf(dy, F, fi.y); fi.z = fmaf(dz, F, fi.z);
