@@ -91,7 +91,6 @@ struct Systems {
     const int4* __restrict__ neighs;
     const int4* __restrict__ neighCell;
     const int4* __restrict__ bkneighs;
-    const int* __restrict__ perm;       // per system: atoms in spatial (Morton) order, local indices
     const float4* __restrict__ apars;
     const float4* __restrict__ bLs;
     const float4* __restrict__ bKs;
@@ -460,8 +459,7 @@ struct SmemLayout {
     // offsets in bytes
     int pos, vel, fasm, fnb, fgrid, REQ, PLQ, ng, ngC, bk, apar, bL, bK, ksp, kpp, fng, red;
     int cwords, cpref, ccnt, clist;     // per-image candidate lists (cutoff + PBC only)
-    int facc;                           // fixed-point force sums of the central image [3 * maxNA] int64
-    int perm, iperm, bblk, total;       // spatial order of the atoms and its inverse (u16), block boxes
+    int facc, total;                    // fixed-point force sums of the central image [3 * maxNA] int64
 };
 
 // number of shifted (non-central) PBC images of the pair term
@@ -499,9 +497,6 @@ __host__ __device__ inline SmemLayout smem_layout(int maxNA, int maxNN, int T, i
     L.ccnt = take(4 * nimg);                // candidates per image
     L.clist = take(2 * nimg * maxNA);       // candidate atom indices per image, ascending
     L.facc = take(8 * 3 * maxNA);
-    L.perm = take(2 * maxNA);
-    L.iperm = take(2 * maxNA);
-    L.bblk = take(4 * 6 * L.nwords);
     L.total = o;
     return L;
 }

@@ -89,13 +89,6 @@ struct Engine {
             sREQ[a] = r; sPLQ[a] = Y.PLQ[aoff + a]; h |= (r.w != 0.f);
             sng[a] = Y.neighs[aoff + a]; sngC[a] = Y.neighCell[aoff + a]; sbk[a] = Y.bkneighs[aoff + a];
         }
-        unsigned short* sperm = at<unsigned short>(L.perm);
-        unsigned short* siperm = at<unsigned short>(L.iperm);
-        for (int k = tid; k < natoms; k += T) {
-            const int a = Y.perm[aoff + k];
-            sperm[k] = (unsigned short)a;
-            siperm[a] = (unsigned short)k;
-        }
         hasH = __syncthreads_or(h) != 0;
         float4* sap = at<float4>(L.apar); float4* sbL = at<float4>(L.bL); float4* sbK = at<float4>(L.bK);
         float4* sks = at<float4>(L.ksp); float4* skp = at<float4>(L.kpp);
@@ -297,13 +290,11 @@ struct Engine {
 
     // own atom i of a tile: position, parameters and its bonded neighbours in
     // the central cell (the excluded j); invalid slots exclude everything
-    struct TileAtom { float4 p, R; int e1, e2, e3, e4, idx; bool v; };
-    // k: slot in the spatial order (perm); the atom is perm[k]
-    __device__ __forceinline__ TileAtom tile_atom(int k, const float4* spos, const float4* sREQ, bool pbc, int central) {
+    struct TileAtom { float4 p, R; int e1, e2, e3, e4; bool v; };
+    __device__ __forceinline__ TileAtom tile_atom(int i, const float4* spos, const float4* sREQ, bool pbc, int central) {
         TileAtom t;
-        t.v = k < natoms;
-        const int ic = t.v ? (int)at<unsigned short>(L.perm)[k] : 0;
-        t.idx = ic;
+        t.v = i < natoms;
+        const int ic = t.v ? i : 0;
         t.p = spos[ic]; t.R = sREQ[ic];
         const int4 ng = at<int4>(L.ng)[ic], ngC = at<int4>(L.ngC)[ic];
         t.e1 = (ngC.x == central || !pbc) ? ng.x : -1;
@@ -315,17 +306,15 @@ struct Engine {
 
     // excluded j-slots of block bj for this lane's atom: all if the atom is a
     // padding slot, padding slots of bj, and the atom's bonded neighbours in bj
-    __device__ __forceinline__ uint32_t tile_mask(const TileAtom& a, int bj) {
+    __device__ __forceinline__ uint32_t tile_mask(const TileAtom& a, int bj) const {
         if (!a.v) return ~0u;
         const int nvalid = natoms - 32 * bj;
         uint32_t m = nvalid >= 32 ? 0u : ~((1u << nvalid) - 1u);
-        const unsigned short* siperm = at<unsigned short>(L.iperm);
         const int e[4] = {a.e1, a.e2, a.e3, a.e4};
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-            if (e[k] < 0) continue;
-            const int d = (int)siperm[e[k]] - 32 * bj;
-            if (d >= 0 && d < 32) m |= 1u << d;
+            const int d = e[k] - 32 * bj;
+            if (e[k] >= 0 && d >= 0 && d < 32) m |= 1u << d;
         }
         return m;
     }
@@ -343,10 +332,10 @@ struct Engine {
         bool ok;
         float e = 0.f;
 #pragma unroll kTileUnroll
-        const unsigned short* sperm = at<unsigned short>(L.perm);
         for (int s = 0; s < 32; s++) {
             const int jl = (lane + s) & 31;
-            const int jc = sperm[min(bj * 32 + jl, natoms - 1)];
+            const int j = bj * 32 + jl;
+            const int jc = min(j, natoms - 1);
             const float4 pj = spos[jc], Rj = sREQ[jc];
             const bool excl = (xm >> jl) & 1u;
             const float dx = pj.x - a.p.x, dy = pj.y - a.p.y, dz = pj.z - a.p.z;
@@ -360,9 +349,9 @@ struct Engine {
             rj.y = __shfl_sync(0xffffffffu, rj.y, nxt);
             rj.z = __shfl_sync(0xffffffffu, rj.z, nxt);
         }
-        if (a.v) fix_add(facc + 3 * a.idx, fi);
+        if (a.v) fix_add(facc + 3 * i, fi);
         const int jo = bj * 32 + lane;
-        if (jo < natoms) fix_add(facc + 3 * (int)sperm[jo], rj);
+        if (jo < natoms) fix_add(facc + 3 * jo, rj);
     }
 
     template <bool HB>
@@ -378,10 +367,9 @@ struct Engine {
         bool ok;
         float e = 0.f;
 #pragma unroll kTileUnroll
-        const unsigned short* sperm = at<unsigned short>(L.perm);
         for (int s = 1; s <= 16; s++) {
             const int jl = (lane + s) & 31;
-            const int jc = sperm[min(b * 32 + jl, natoms - 1)];
+            const int jc = min(b * 32 + jl, natoms - 1);
             const float4 pj = spos[jc], Rj = sREQ[jc];
             const bool excl = ((xm >> jl) & 1u) || (s == 16 && lane >= 16);
             const float dx = pj.x - a.p.x, dy = pj.y - a.p.y, dz = pj.z - a.p.z;
@@ -394,7 +382,7 @@ struct Engine {
             fi.y += __shfl_sync(0xffffffffu, -dy * F, src);
             fi.z += __shfl_sync(0xffffffffu, -dz * F, src);
         }
-        if (a.v) fix_add(facc + 3 * a.idx, fi);
+        if (a.v) fix_add(facc + 3 * i, fi);
     }
 
     // work units: each off-diagonal tile, and pairs of diagonal tiles (equal
@@ -409,18 +397,7 @@ struct Engine {
             if (u < noff) {
                 int bi = 0, rem = u;
                 while (rem >= B - 1 - bi) { rem -= B - 1 - bi; bi++; }
-                const int bj = bi + 1 + rem;
-                if (P.Rc2 > 0.f) {          // blocks whose boxes are beyond the cutoff: nothing to do
-                    const float* bb = at<float>(L.bblk);
-                    float g2 = 0.f;
-#pragma unroll
-                    for (int k = 0; k < 3; k++) {
-                        const float g = fmaxf(0.f, fmaxf(bb[6 * bj + k] - bb[6 * bi + 3 + k], bb[6 * bi + k] - bb[6 * bj + 3 + k]));
-                        g2 = fmaf(g, g, g2);
-                    }
-                    if (g2 >= P.Rc2) continue;
-                }
-                off_tile<HB>(bi, bj, spos, sREQ, pbc, central, facc, ec);
+                off_tile<HB>(bi, bi + 1 + rem, spos, sREQ, pbc, central, facc, ec);
             } else {
                 const int d = 2 * (u - noff);
                 diag_tile<HB>(d, spos, sREQ, pbc, central, facc, ec);
@@ -535,19 +512,6 @@ struct Engine {
             // central image: every unordered pair once, into fixed-point sums
             long long* facc = at<long long>(L.facc);
             for (int a = tid; a < 3 * natoms; a += T) facc[a] = 0;
-            if (P.Rc2 > 0.f) {              // bounding box of every 32-atom block of the spatial order
-                float* bb = at<float>(L.bblk);
-                const unsigned short* sperm = at<unsigned short>(L.perm);
-                for (int blk = warp; blk < (natoms + 31) / 32; blk += L.nwarps) {
-                    const float4 p = spos[sperm[min(blk * 32 + lane, natoms - 1)]];
-                    const float mn[3] = {wmin(p.x), wmin(p.y), wmin(p.z)};
-                    const float mx[3] = {wmax(p.x), wmax(p.y), wmax(p.z)};
-                    if (lane == 0) {
-#pragma unroll
-                        for (int k = 0; k < 3; k++) { bb[6 * blk + k] = mn[k]; bb[6 * blk + 3 + k] = mx[k]; }
-                    }
-                }
-            }
             __syncthreads();
             {
                 float ec = 0.f;

@@ -98,7 +98,7 @@ struct World {
     std::vector<int4> desc;
     std::vector<double> orig;      // [nsys*3]
     DBuf<int4> d_desc; DBuf<int> d_nnode; DBuf<float> d_lvec; DBuf<float4> d_gorg;
-    DBuf<float4> d_REQ, d_PLQ; DBuf<int4> d_ng, d_ngC, d_bk; DBuf<int> d_perm;
+    DBuf<float4> d_REQ, d_PLQ; DBuf<int4> d_ng, d_ngC, d_bk;
     DBuf<float4> d_apar, d_bL, d_bK, d_ksp, d_kpp;
     DBuf<float4> d_pos, d_vel, d_force, d_pos0, d_vel0;
     DBuf<double4> d_fire, d_fire0, d_energy;
@@ -189,7 +189,6 @@ Systems make_systems() {
     Y.nsys = W.nsys;
     Y.desc = W.d_desc.p; Y.nnode = W.d_nnode.p; Y.lvec = W.d_lvec.p; Y.gorg = W.d_gorg.p;
     Y.REQ = W.d_REQ.p; Y.PLQ = W.d_PLQ.p; Y.neighs = W.d_ng.p; Y.neighCell = W.d_ngC.p; Y.bkneighs = W.d_bk.p;
-    Y.perm = W.d_perm.p;
     Y.apars = W.d_apar.p; Y.bLs = W.d_bL.p; Y.bKs = W.d_bK.p; Y.Ksp = W.d_ksp.p; Y.Kpp = W.d_kpp.p;
     Y.pos = W.d_pos.p; Y.vel = W.d_vel.p; Y.force = W.d_force.p; Y.fire = W.d_fire.p;
     Y.status = W.d_status.p; Y.nsteps = W.d_nsteps.p; Y.fconv = W.d_fconv.p; Y.energy = W.d_energy.p;
@@ -504,7 +503,6 @@ int mmff_systems_upload(int nsys, const int* natoms, const int* nnode, const dou
     W.orig.assign(3 * nsys, 0.0);
     std::vector<float4> hpos(NV), hvel(NV), hREQ(NA), hPLQ(NA), hap(NN), hbL(NN), hbK(NN), hks(NN), hkp(NN), hgorg(nsys);
     std::vector<int4> hng(NA), hngC(NA), hbk(NA);
-    std::vector<int> hperm(NA);
     std::vector<float> hlv(9 * nsys);
     std::vector<double4> hfire(nsys);
     const double sqk = std::sqrt(14.3996448915);
@@ -531,24 +529,6 @@ int mmff_systems_upload(int nsys, const int* natoms, const int* nnode, const dou
             const int* gc = neighCell + 4 * (a0 + i); hngC[a0 + i] = make_int4(gc[0], gc[1], gc[2], gc[3]);
             const int* b = bkneighs + 4 * (a0 + i); hbk[a0 + i] = make_int4(b[0], b[1], b[2], b[3]);
         }
-        // spatial order of the atoms (Morton code of 2.5 A cells of the start
-        // geometry): 32-atom blocks in this order are compact, so the pair
-        // kernels can skip block pairs beyond the cutoff
-        {
-            double mn[3] = {1e300, 1e300, 1e300};
-            for (int i = 0; i < na; i++) for (int k = 0; k < 3; k++) mn[k] = std::min(mn[k], pos[3 * (v0 + i) + k]);
-            std::vector<std::pair<unsigned long long, int>> key(na);
-            for (int i = 0; i < na; i++) {
-                unsigned long long code = 0;
-                unsigned q[3];
-                for (int k = 0; k < 3; k++) q[k] = (unsigned)std::min(1023.0, (pos[3 * (v0 + i) + k] - mn[k]) / 2.5);
-                for (int b = 9; b >= 0; b--)
-                    for (int k = 0; k < 3; k++) code = (code << 1) | ((q[k] >> b) & 1u);
-                key[i] = {code, i};
-            }
-            std::sort(key.begin(), key.end());
-            for (int i = 0; i < na; i++) hperm[a0 + i] = key[i].second;
-        }
         for (int i = 0; i < nn; i++) {
             auto f4 = [&](const double* a) { return make_float4((float)a[4 * (n0 + i)], (float)a[4 * (n0 + i) + 1], (float)a[4 * (n0 + i) + 2], (float)a[4 * (n0 + i) + 3]); };
             hap[n0 + i] = f4(apars); hbL[n0 + i] = f4(bLs); hbK[n0 + i] = f4(bKs); hks[n0 + i] = f4(Ksp); hkp[n0 + i] = f4(Kpp);
@@ -559,7 +539,7 @@ int mmff_systems_upload(int nsys, const int* natoms, const int* nnode, const dou
     }
     std::vector<int4> hdesc = W.desc;
     if (upload(W.d_desc, hdesc) || upload(W.d_nnode, W.nnode) || upload(W.d_lvec, hlv) || upload(W.d_gorg, hgorg) ||
-        upload(W.d_REQ, hREQ) || upload(W.d_PLQ, hPLQ) || upload(W.d_ng, hng) || upload(W.d_ngC, hngC) || upload(W.d_perm, hperm) ||
+        upload(W.d_REQ, hREQ) || upload(W.d_PLQ, hPLQ) || upload(W.d_ng, hng) || upload(W.d_ngC, hngC) ||
         upload(W.d_bk, hbk) || upload(W.d_apar, hap) || upload(W.d_bL, hbL) || upload(W.d_bK, hbK) ||
         upload(W.d_ksp, hks) || upload(W.d_kpp, hkp) || upload(W.d_pos, hpos) || upload(W.d_vel, hvel) ||
         upload(W.d_pos0, hpos) || upload(W.d_vel0, hvel) || upload(W.d_fire, hfire) || upload(W.d_fire0, hfire))
