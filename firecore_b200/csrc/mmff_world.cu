@@ -304,6 +304,22 @@ int build_buckets() {
     return 0;
 }
 
+// Page-locked host staging for the per-call state copies (positions and
+// velocities in, state out), so the transfers run at full PCIe/C2C rate.
+struct PinnedBuf {
+    float4* p = nullptr; size_t n = 0;
+    int ensure(size_t cnt) {
+        if (cnt <= n && p) return 0;
+        if (p) cudaFreeHost(p);
+        p = nullptr; n = 0;
+        if (cudaHostAlloc(reinterpret_cast<void**>(&p), cnt * sizeof(float4), cudaHostAllocDefault) != cudaSuccess)
+            return fail("cudaHostAlloc(%zu B) failed", cnt * sizeof(float4));
+        n = cnt;
+        return 0;
+    }
+};
+PinnedBuf g_stage_a, g_stage_b;
+
 template <class X> int upload(DBuf<X>& d, const std::vector<X>& h) {
     if (d.ensure(h.size())) return -1;
     if (!h.empty()) CK(cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(X), cudaMemcpyHostToDevice, W.stream));
@@ -569,7 +585,9 @@ int mmff_systems_restore(void) {
 int mmff_systems_set_state(const double* pos, const double* vel, int reset_fire) {
     if (ensure_ready()) return -1;
     if (!W.nsys) return fail("no systems uploaded");
-    std::vector<float4> hpos(W.NV), hvel(W.NV);
+    if (g_stage_a.ensure(W.NV) || g_stage_b.ensure(W.NV)) return -1;
+    float4* hpos = g_stage_a.p;
+    float4* hvel = g_stage_b.p;
     for (int s = 0; s < W.nsys; s++) {
         const int v0 = W.desc[s].z, na = W.natoms[s], nn = W.nnode[s];
         const double* c = W.orig.data() + 3 * s;
@@ -581,8 +599,8 @@ int mmff_systems_set_state(const double* pos, const double* vel, int reset_fire)
             hvel[v0 + i] = v ? make_float4((float)v[0], (float)v[1], (float)v[2], 0.f) : make_float4(0, 0, 0, 0);
         }
     }
-    CK(cudaMemcpyAsync(W.d_pos.p, hpos.data(), W.NV * sizeof(float4), cudaMemcpyHostToDevice, W.stream));
-    CK(cudaMemcpyAsync(W.d_vel.p, hvel.data(), W.NV * sizeof(float4), cudaMemcpyHostToDevice, W.stream));
+    CK(cudaMemcpyAsync(W.d_pos.p, hpos, W.NV * sizeof(float4), cudaMemcpyHostToDevice, W.stream));
+    CK(cudaMemcpyAsync(W.d_vel.p, hvel, W.NV * sizeof(float4), cudaMemcpyHostToDevice, W.stream));
     if (reset_fire) {
         std::vector<double4> hf(W.nsys, make_double4(W.fire[0], W.fire[2], 0.0, 0.0));
         CK(cudaMemcpyAsync(W.d_fire.p, hf.data(), W.nsys * sizeof(double4), cudaMemcpyHostToDevice, W.stream));
@@ -829,14 +847,17 @@ int mmff_get_energies(double* E) {
 int mmff_get_state(double* pos, double* vel, double* fire, int* status, int* nsteps, double* fconv) {
     if (mmff_sync()) return -1;
     if (pos || vel) {
-        std::vector<float4> hp(W.NV), hv(W.NV);
-        CK(cudaMemcpy(hp.data(), W.d_pos.p, W.NV * sizeof(float4), cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(hv.data(), W.d_vel.p, W.NV * sizeof(float4), cudaMemcpyDeviceToHost));
+        if (g_stage_a.ensure(W.NV) || g_stage_b.ensure(W.NV)) return -1;
+        const float4* hp = g_stage_a.p;
+        const float4* hv = g_stage_b.p;
+        CK(cudaMemcpyAsync(g_stage_a.p, W.d_pos.p, W.NV * sizeof(float4), cudaMemcpyDeviceToHost, W.stream));
+        if (vel) CK(cudaMemcpyAsync(g_stage_b.p, W.d_vel.p, W.NV * sizeof(float4), cudaMemcpyDeviceToHost, W.stream));
+        CK(cudaStreamSynchronize(W.stream));
         for (int s = 0; s < W.nsys; s++) {
             const int v0 = W.desc[s].z, na = W.natoms[s], nn = W.nnode[s];
             const double* c = W.orig.data() + 3 * s;
             for (int i = 0; i < na + nn; i++) {
-                const float4 p = hp[v0 + i], v = hv[v0 + i];
+                const float4 p = hp[v0 + i], v = vel ? hv[v0 + i] : make_float4(0.f, 0.f, 0.f, 0.f);
                 if (pos) {
                     if (i < na) { pos[3 * (v0 + i)] = c[0] + p.x; pos[3 * (v0 + i) + 1] = c[1] + p.y; pos[3 * (v0 + i) + 2] = c[2] + p.z; }
                     else { pos[3 * (v0 + i)] = p.x; pos[3 * (v0 + i) + 1] = p.y; pos[3 * (v0 + i) + 2] = p.z; }
