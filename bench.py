@@ -231,6 +231,7 @@ def run_ours(args):
     pair_tf = PAIR_FLOPS * attr_pairs / t_pair / 1e12 if t_pair > 0 else None
     grid_term_gbs = GRID_BYTES * attr_grid / t_grid / 1e9 if t_grid > 0 else None
     out = None
+    parity = parity_subset(w, batch, sub, C) if rank == 0 else None
     if rank == 0:
         cpu = cpu_baseline(batch, sub, C, args) if not args.no_cpu else None
         nconv0 = int((st0["status"] == 1).sum())
@@ -264,7 +265,7 @@ def run_ours(args):
                                        "time_ms": 1e3 * t_grid,
                                        "method": "200-step relax with all terms minus without GridFF"},
                          "term_times_ms": attr_t},
-            "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "parity_vs_oracle": parity,
             "buckets": w.buckets(), "relax_graph": True,
             "autotune": {"seconds": tune_s, "chosen": {str(k): v for k, v in w.tuning().items()},
                          "candidates": [[r["size_class"], r["kind"], r["threads"], r["pair_lanes"],
@@ -329,6 +330,28 @@ def term_attribution(w, lib, nsteps=200):
 def _lib_ptr(a):
     from firecore_b200 import _lib
     return _lib.ptr(a)
+
+
+def parity_subset(w, batch, sub, C, nsub=64):
+    """Per-atom forces and per-system energies of the device at the final
+    geometries of the first nsub systems, against the FP64 oracle evaluated at
+    the same positions (untimed)."""
+    from oracle import oracle as O
+    F, E = w.eval(True)
+    pos = w.state()["pos"]
+    idx = list(range(min(nsub, batch.nsys)))
+    a, n, v = batch.offsets()
+    sb = batch.subset(idx)
+    rows = np.concatenate([np.arange(v[s], v[s + 1]) for s in idx])
+    Fo, Eo = O.eval_forces(sb, O.make_params(sub.grid, npbc=(1, 1, 0), Rcut=RCUT), C, pos=pos[rows])
+    Fd = F[rows]
+    _, _, vs = sb.offsets()
+    ferr = [float(np.abs(Fd[vs[k]:vs[k + 1]] - Fo[vs[k]:vs[k + 1]]).max() / max(np.abs(Fo[vs[k]:vs[k + 1]]).max(), 1e-12))
+            for k in range(len(idx))]
+    eerr = np.abs(E[idx, 3] - Eo[:, 3]) / sb.natoms
+    return {"systems": len(idx), "max_force_rel_err": max(ferr), "median_force_rel_err": float(np.median(ferr)),
+            "max_energy_err_eV_per_atom": float(eerr.max()), "median_energy_err_eV_per_atom": float(np.median(eerr)),
+            "reference": "FP64 oracle (restatement pinned to FireCore's compiled run_no_omp physics)"}
 
 
 def cpu_baseline(batch, sub, C, args):
