@@ -190,6 +190,7 @@ struct LegacyWorld {
     // thermal drive of init(T, gamma) (MolWorld_sp3_multi's TDrive): MDloop runs
     // Langevin dynamics instead of FIRE when both are > 0
     double T = 0.0, gamma = 0.0;
+    bool md_set = false;          // Langevin parameters passed to the device world
     // host mirrors (pyBall/MMFF_multi.py:238-256 shapes)
     std::vector<float> atoms, aforces, avel, constr, REQs, MMpars, BLs, BKs, Ksp, Kpp, lvecs, ilvecs, pbcshifts;
     std::vector<int> gneighs, gneighCell, gbkNeighs;
@@ -357,7 +358,7 @@ void* init(int nSys, char* xyz_name, char* surf_name, char* smile_name, bool bMM
            int nExplore, int nRelax, double pos_kick, double vel_kick, int GridFF) {
     (void)smile_name; (void)bMMFF; (void)bEpairs; (void)sElementTypes; (void)sAtomTypes; (void)sBondTypes; (void)sAngleTypes;
     (void)nExplore; (void)nRelax; (void)pos_kick; (void)vel_kick;
-    L.T = T; L.gamma = gamma;
+    L.T = T; L.gamma = gamma; L.md_set = false;
     if (nSys < 1 || !xyz_name) { set_error("init: need nSys >= 1 and an xyz file"); return nullptr; }
     if (mmff_init_device(0)) { set_error(std::string("init: ") + mmff_last_error()); return nullptr; }
     XYZ X;
@@ -468,9 +469,8 @@ int run(int nstepMax, double dt, double Fconv, int ialg, double* outE, double* o
 void MDloop(int perframe, double Ftol, int iParalel, int perVF) {
     (void)perVF;
     if (L.ready && L.T > 0 && L.gamma > 0) {
-        static bool md_set = false;
-        if (!md_set && mmff_set_md(L.fire[0], L.gamma, L.T, 12345ull)) { set_error(mmff_last_error()); return; }
-        md_set = true;
+        if (!L.md_set && mmff_set_md(L.fire[0], L.gamma, L.T, 12345ull)) { set_error(mmff_last_error()); return; }
+        L.md_set = true;
         if (mmff_md(perframe) || mmff_sync()) { set_error(mmff_last_error()); return; }
         if (download_all(true, true)) return;
         copy_sys_to_cpu(L.iSystemCur);

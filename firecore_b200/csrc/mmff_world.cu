@@ -214,16 +214,17 @@ int size_class(int na) {
 // is per function, and several buckets (or autotuner candidates) can share one
 // kernel instantiation, so it only ever grows.
 int set_smem_limit(void* fn, int bytes) {
-    static std::vector<std::pair<void*, int>> seen;
+    struct Seen { void* fn; int device; int bytes; };
+    static std::vector<Seen> seen;
     for (auto& e : seen) {
-        if (e.first != fn) continue;
-        if (bytes <= e.second) return 0;
+        if (e.fn != fn || e.device != W.device) continue;
+        if (bytes <= e.bytes) return 0;
         CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-        e.second = bytes;
+        e.bytes = bytes;
         return 0;
     }
     CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-    seen.emplace_back(fn, bytes);
+    seen.push_back({fn, W.device, bytes});
     return 0;
 }
 
