@@ -64,8 +64,10 @@ def workload(rank, nsys, kind="replicas"):
 
 def workload_name(args):
     if args.workload == "uneven":
-        return (f"{args.nsys} distinct molecules, 20-400 atoms log-uniform (CSR, size buckets, per-bucket work "
-                f"queues) on NaCl slab, GridFF 226x226x200, Rcut {RCUT} A, Fmax<{FCONV}, <= {MAXSTEPS} FIRE steps")
+        return (f"queue of {args.nsys} distinct molecules, 20-400 atoms log-uniform (CSR, size buckets, one "
+                f"persistent kernel per bucket claiming systems from its work queue: converged systems retire and "
+                f"their CTA slots refill) on NaCl slab, GridFF 226x226x200, Rcut {RCUT} A, Fmax<{FCONV}, "
+                f"<= {MAXSTEPS} FIRE steps")
     return (f"{args.nsys} replicas x 60-atom molecule on NaCl slab, GridFF 226x226x200, "
             f"Rcut {RCUT} A, Fmax<{FCONV}, <= {MAXSTEPS} FIRE steps")
 
@@ -233,7 +235,9 @@ def run_ours(args):
     out = None
     parity = parity_subset(w, batch, sub, C) if rank == 0 else None
     if rank == 0:
-        cpu = cpu_baseline(batch, sub, C, args) if not args.no_cpu else None
+        cpu = cpu_baseline(batch, sub, C, args, st0) if not args.no_cpu else None
+        if cpu:
+            parity["relaxed_geometry"] = cpu.pop("geometry")
         nconv0 = int((st0["status"] == 1).sum())
         steps_conv = st0["nsteps"][st0["status"] == 1]
         out = {
@@ -333,30 +337,61 @@ def _lib_ptr(a):
 
 
 def parity_subset(w, batch, sub, C, nsub=64):
-    """Per-atom forces and per-system energies of the device at the final
-    geometries of the first nsub systems, against the FP64 oracle evaluated at
-    the same positions (untimed)."""
+    """Device against the FP64 oracle on the first nsub systems (untimed).
+    Forces at the starting geometries (|F| ~ 1-10 eV/A): per system the largest
+    per-atom force error over the largest force.  At the final geometries the
+    forces are ~Fconv, so their error is stated in eV/A, and the energies in
+    eV/atom.  Leaves the device state at the starting geometries."""
     from oracle import oracle as O
-    F, E = w.eval(True)
-    pos = w.state()["pos"]
     idx = list(range(min(nsub, batch.nsys)))
     a, n, v = batch.offsets()
     sb = batch.subset(idx)
-    rows = np.concatenate([np.arange(v[s], v[s + 1]) for s in idx])
-    Fo, Eo = O.eval_forces(sb, O.make_params(sub.grid, npbc=(1, 1, 0), Rcut=RCUT), C, pos=pos[rows])
-    Fd = F[rows]
     _, _, vs = sb.offsets()
-    ferr = [float(np.abs(Fd[vs[k]:vs[k + 1]] - Fo[vs[k]:vs[k + 1]]).max() / max(np.abs(Fo[vs[k]:vs[k + 1]]).max(), 1e-12))
-            for k in range(len(idx))]
+    rows = np.concatenate([np.arange(v[s], v[s + 1]) for s in idx])
+    P = O.make_params(sub.grid, npbc=(1, 1, 0), Rcut=RCUT)
+    F, E = w.eval(True)
+    pos = w.state()["pos"]
+    Fo, Eo = O.eval_forces(sb, P, C, pos=pos[rows])
+    Fd = F[rows]
+    fabs = [float(np.abs(Fd[vs[k]:vs[k + 1]] - Fo[vs[k]:vs[k + 1]]).max()) for k in range(len(idx))]
     eerr = np.abs(E[idx, 3] - Eo[:, 3]) / sb.natoms
-    return {"systems": len(idx), "max_force_rel_err": max(ferr), "median_force_rel_err": float(np.median(ferr)),
-            "max_energy_err_eV_per_atom": float(eerr.max()), "median_energy_err_eV_per_atom": float(np.median(eerr)),
+    w.restore()
+    F0, _ = w.eval(True)
+    Fo0, _ = O.eval_forces(sb, P, C, pos=batch.pos[rows])
+    F0 = F0[rows]
+    frel = [float(np.linalg.norm(F0[vs[k]:vs[k + 1]] - Fo0[vs[k]:vs[k + 1]], axis=1).max()
+                  / max(np.linalg.norm(Fo0[vs[k]:vs[k + 1]], axis=1).max(), 1e-12)) for k in range(len(idx))]
+    return {"systems": len(idx),
+            "start_max_force_rel_err": max(frel), "start_median_force_rel_err": float(np.median(frel)),
+            "final_max_force_abs_err_eV_per_A": max(fabs),
+            "final_max_energy_err_eV_per_atom": float(eerr.max()),
+            "final_median_energy_err_eV_per_atom": float(np.median(eerr)),
             "reference": "FP64 oracle (restatement pinned to FireCore's compiled run_no_omp physics)"}
 
 
-def cpu_baseline(batch, sub, C, args):
+def geometry_parity(batch, st0, r, nsample):
+    """Relaxed geometries of the device (st0) against the oracle's FP64
+    relaxation of the same first nsample systems (r): atom RMSD per system
+    converged in both."""
+    _, _, v = batch.offsets()
+    both = [s for s in range(nsample) if st0["status"][s] == 1 and r["converged"][s] == 1]
+    _, _, vs = batch.subset(range(nsample)).offsets()
+    rmsd = []
+    for s in both:
+        na = int(batch.natoms[s])
+        d = st0["pos"][v[s]:v[s] + na, :3] - r["pos"][vs[s]:vs[s] + na, :3]
+        rmsd.append(float(np.sqrt((d ** 2).sum(1).mean())))
+    rmsd = np.array(rmsd)
+    return {"systems_converged_in_both": len(both),
+            "fraction_rmsd_le_1e-3_A": float((rmsd <= 1e-3).mean()) if len(rmsd) else None,
+            "median_rmsd_A": float(np.median(rmsd)) if len(rmsd) else None,
+            "max_rmsd_A": float(rmsd.max()) if len(rmsd) else None}
+
+
+def cpu_baseline(batch, sub, C, args, st0):
     """The FP64 oracle (OpenMP over systems) on a bounded sample of the same
-    workload, same parameters (10 A cutoff, force clamp, Fmax criterion)."""
+    workload, same parameters (10 A cutoff, force clamp, Fmax criterion).  Its
+    relaxed geometries are compared with the device's (st0) as well."""
     from oracle import oracle as O
     model, ncores = cpu_info()
     nsample = int(min(batch.nsys, max(64, 32 * ncores), 1024))
@@ -370,7 +405,8 @@ def cpu_baseline(batch, sub, C, args):
     dt = time.perf_counter() - t0
     conv = int((r["converged"] == 1).sum())
     return {"value": conv / dt, "unit": UNIT, "cores": ncores, "kind": "port",
-            "sample": f"{nsample} of the systems, full relaxation each ({conv} converged, {dt:.1f} s), CPU: {model}"}
+            "sample": f"{nsample} of the systems, full relaxation each ({conv} converged, {dt:.1f} s), CPU: {model}",
+            "geometry": geometry_parity(batch, st0, r, nsample)}
 
 
 # --------------------------------------------------------------------------- learned vs plain
@@ -560,7 +596,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--nsys", type=int, default=None, help="systems per GPU (default 4096; 16384 with --workload learned)")
+    ap.add_argument("--nsys", type=int, default=None, help="systems per GPU (default 4096 replicas; a 32768-system queue uneven; 16384 learned)")
     ap.add_argument("--workload", default="replicas", choices=["replicas", "uneven", "learned"])
     ap.add_argument("--train-sys", type=int, default=1024, help="--workload learned: systems whose trajectories train the network")
     ap.add_argument("--train-steps", type=int, default=2000)
@@ -571,7 +607,7 @@ def main():
     args = ap.parse_args()
     MAXSTEPS = args.maxsteps
     if args.nsys is None:
-        args.nsys = 16384 if args.workload == "learned" else 4096
+        args.nsys = {"learned": 16384, "uneven": 32768}.get(args.workload, 4096)
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "learned":
