@@ -468,28 +468,44 @@ __host__ __device__ inline int shifted_images(int flags, const int* npbc) {
     return (2 * npbc[0] + 1) * (2 * npbc[1] + 1) * (2 * npbc[2] + 1) - 1;
 }
 
-// nimg: shifted images that get candidate lists (0: none)
-__host__ __device__ inline SmemLayout smem_layout(int maxNA, int maxNN, int T, int nimg) {
+// Layouts above this size would hold one CTA per SM.  Above it, the arrays
+// read once per atom (or node) per step stay in global memory and are read
+// through L1: neighbours, their cells, back-neighbour slots, GridFF
+// coefficients and the node parameters (offset -1 in the layout).  That
+// brings a 400-atom system under half of the SM's shared memory.  Only
+// blocks of >= 256 threads take it (smaller blocks compile without the
+// global-memory branch).
+constexpr int kCompactAbove = 112 * 1024;
+constexpr int kCompactMinThreads = 256;
+
+// Image tiles are compiled into blocks of >= 128 threads only: the 64-thread
+// blocks serve molecules of <= 64 atoms, whose images reach a few edge atoms
+// (short candidate lists, ordered rows), and without the tile code there the
+// code of their central tiles stays as it is.
+constexpr int kImageTileMinThreads = 128;
+
+__host__ __device__ inline SmemLayout smem_layout_(int maxNA, int maxNN, int T, int nimg, bool compact) {
     SmemLayout L;
     L.maxNA = maxNA; L.maxNN = maxNN; L.maxNV = maxNA + maxNN; L.nwarps = T / 32;
     L.nimg = nimg; L.nwords = (maxNA + 31) / 32;
     int o = 0;
     auto take = [&](int bytes) { int r = o; o += (bytes + 15) & ~15; return r; };
+    auto opt = [&](int bytes) { return compact ? -1 : take(bytes); };
     L.pos = take(16 * L.maxNV);
     L.vel = take(16 * L.maxNV);
     L.fasm = take(16 * L.maxNV);
     L.fnb = take(16 * maxNA);
     L.fgrid = take(16 * maxNA);
     L.REQ = take(16 * maxNA);
-    L.PLQ = take(16 * maxNA);
-    L.ng = take(16 * maxNA);
-    L.ngC = take(16 * maxNA);
-    L.bk = take(16 * maxNA);
-    L.apar = take(16 * maxNN);
-    L.bL = take(16 * maxNN);
-    L.bK = take(16 * maxNN);
-    L.ksp = take(16 * maxNN);
-    L.kpp = take(16 * maxNN);
+    L.PLQ = opt(16 * maxNA);
+    L.ng = opt(16 * maxNA);
+    L.ngC = opt(16 * maxNA);
+    L.bk = opt(16 * maxNA);
+    L.apar = opt(16 * maxNN);
+    L.bL = opt(16 * maxNN);
+    L.bK = opt(16 * maxNN);
+    L.ksp = opt(16 * maxNN);
+    L.kpp = opt(16 * maxNN);
     L.fng = take(16 * 8 * maxNN);
     L.red = take(128 * L.nwarps + 64);     // per warp: 4 doubles (32 B) at 0, bbox 6 floats at 64*nwarps
     L.cwords = take(4 * nimg * L.nwords);   // candidate bit words per image
@@ -499,6 +515,12 @@ __host__ __device__ inline SmemLayout smem_layout(int maxNA, int maxNN, int T, i
     L.facc = take(8 * 3 * maxNA);
     L.total = o;
     return L;
+}
+
+// nimg: shifted images that get candidate lists (0: none)
+__host__ __device__ inline SmemLayout smem_layout(int maxNA, int maxNN, int T, int nimg) {
+    const SmemLayout L = smem_layout_(maxNA, maxNN, T, nimg, false);
+    return (T >= kCompactMinThreads && L.total > kCompactAbove) ? smem_layout_(maxNA, maxNN, T, nimg, true) : L;
 }
 
 // ---- shared-memory carve-up of one warp-per-system region (byte offsets)

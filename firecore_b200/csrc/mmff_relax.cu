@@ -68,6 +68,18 @@ struct Engine {
         tid = threadIdx.x; lane = tid & 31; warp = tid >> 5;
     }
     template <class X> __device__ __forceinline__ X* at(int off) { return reinterpret_cast<X*>(sm + off); }
+    // per-atom / per-node arrays that a compact layout leaves in global memory
+    static constexpr bool kMayCompact = T >= kCompactMinThreads;
+    __device__ __forceinline__ bool compact() const { return kMayCompact && L.ng < 0; }
+    __device__ __forceinline__ int4 ngs(int a) { return compact() ? __ldg(Y.neighs + aoff + a) : at<int4>(L.ng)[a]; }
+    __device__ __forceinline__ int4 ngc(int a) { return compact() ? __ldg(Y.neighCell + aoff + a) : at<int4>(L.ngC)[a]; }
+    __device__ __forceinline__ int4 bks(int a) { return compact() ? __ldg(Y.bkneighs + aoff + a) : at<int4>(L.bk)[a]; }
+    __device__ __forceinline__ float4 plq(int a) { return compact() ? __ldg(Y.PLQ + aoff + a) : at<float4>(L.PLQ)[a]; }
+    __device__ __forceinline__ float4 npar(int off, const float4* g, int n) {
+        return compact() ? __ldg(g + noff + n) : at<float4>(off)[n];
+    }
+    // image tiles for long candidate lists (else ordered rows only)
+    static constexpr bool kImgTiles = T >= kImageTileMinThreads;
 
     __device__ void load(int s) {
         isys = s;
@@ -81,21 +93,26 @@ struct Engine {
         gorg = make_float3(g.x, g.y, g.z);
         float4* spos = at<float4>(L.pos); float4* svel = at<float4>(L.vel);
         for (int v = tid; v < nvecs; v += T) { spos[v] = Y.pos[voff + v]; svel[v] = Y.vel[voff + v]; }
-        float4* sREQ = at<float4>(L.REQ); float4* sPLQ = at<float4>(L.PLQ);
-        int4* sng = at<int4>(L.ng); int4* sngC = at<int4>(L.ngC); int4* sbk = at<int4>(L.bk);
+        float4* sREQ = at<float4>(L.REQ);
+        const bool full = !compact();         // else topology stays in global memory
         int h = 0;
         for (int a = tid; a < natoms; a += T) {
             const float4 r = Y.REQ[aoff + a];
-            sREQ[a] = r; sPLQ[a] = Y.PLQ[aoff + a]; h |= (r.w != 0.f);
-            sng[a] = Y.neighs[aoff + a]; sngC[a] = Y.neighCell[aoff + a]; sbk[a] = Y.bkneighs[aoff + a];
+            sREQ[a] = r; h |= (r.w != 0.f);
+            if (full) {
+                at<float4>(L.PLQ)[a] = Y.PLQ[aoff + a];
+                at<int4>(L.ng)[a] = Y.neighs[aoff + a];
+                at<int4>(L.ngC)[a] = Y.neighCell[aoff + a];
+                at<int4>(L.bk)[a] = Y.bkneighs[aoff + a];
+            }
         }
         hasH = __syncthreads_or(h) != 0;
-        float4* sap = at<float4>(L.apar); float4* sbL = at<float4>(L.bL); float4* sbK = at<float4>(L.bK);
-        float4* sks = at<float4>(L.ksp); float4* skp = at<float4>(L.kpp);
-        for (int n = tid; n < nnode; n += T) {
-            sap[n] = Y.apars[noff + n]; sbL[n] = Y.bLs[noff + n]; sbK[n] = Y.bKs[noff + n];
-            sks[n] = Y.Ksp[noff + n]; skp[n] = Y.Kpp[noff + n];
-        }
+        if (full)
+            for (int n = tid; n < nnode; n += T) {
+                at<float4>(L.apar)[n] = Y.apars[noff + n]; at<float4>(L.bL)[n] = Y.bLs[noff + n];
+                at<float4>(L.bK)[n] = Y.bKs[noff + n]; at<float4>(L.ksp)[n] = Y.Ksp[noff + n];
+                at<float4>(L.kpp)[n] = Y.Kpp[noff + n];
+            }
     }
 
     // bounding box of the atoms (all threads end with the same box); needs a barrier inside
@@ -296,7 +313,7 @@ struct Engine {
         t.v = i < natoms;
         const int ic = t.v ? i : 0;
         t.p = spos[ic]; t.R = sREQ[ic];
-        const int4 ng = at<int4>(L.ng)[ic], ngC = at<int4>(L.ngC)[ic];
+        const int4 ng = ngs(ic), ngC = ngc(ic);
         t.e1 = (ngC.x == central || !pbc) ? ng.x : -1;
         t.e2 = (ngC.y == central || !pbc) ? ng.y : -1;
         t.e3 = (ngC.z == central || !pbc) ? ng.z : -1;
@@ -385,23 +402,174 @@ struct Engine {
         if (a.v) fix_add(facc + 3 * i, fi);
     }
 
-    // work units: each off-diagonal tile, and pairs of diagonal tiles (equal
-    // cost), dealt round-robin to the warps
+    // position of atom e in the candidate list of image k, or -1
+    __device__ __forceinline__ int cand_slot(int k, int e) {
+        if (e < 0) return -1;
+        const int w = k * L.nwords + (e >> 5);
+        const uint32_t m = at<uint32_t>(L.cwords)[w];
+        if (!((m >> (e & 31)) & 1u)) return -1;
+        return at<int>(L.cpref)[w] + __popc(m & ((1u << (e & 31)) - 1u));
+    }
+
+    // ---- shifted images, each unordered image pair once -----------------------
+    // Atom i meets image +k of atom j exactly when atom j meets image -k of
+    // atom i, with the opposite force.  So for long candidate lists only the
+    // images k < nimg / 2 are visited (image nimg-1-k is the mirror of k), as
+    // 32 x 32 tiles of (candidates i of image -k) x (candidates j of image +k),
+    // each pair once, the reaction on j rotating through the lanes as in
+    // off_tile.  Excluded (NBFF::evalLJQs_ng4_PBC_atom, NBFF.h:590-607): i
+    // itself, and the bonded neighbours of i whose cell is this image; both
+    // are symmetric under the mirror.  k: image index without the central
+    // one (iz, iy, ix order).
     template <bool HB>
-    __device__ void central_tiles(const float4* spos, const float4* sREQ, bool pbc, int central, long long* facc,
-                                  float& ec) {
+    __device__ void image_tile(int k, int ti, int tj, const float4* spos, const float4* sREQ, long long* facc,
+                               float& ec) {
+        const bool CUT = P.Rc2 > 0.f;
+        const float Rc2 = CUT ? P.Rc2 : 3.0e38f, kq = P.kq_rc2;
+        const float rc = CUT ? sqrtf(1.f / kq) : 0.f;
+        const int nxi = 2 * P.npbc[0] + 1, nyi = 2 * P.npbc[1] + 1;
+        const int ipbc = k;                                   // k < central: same index with the central one
+        const int ix = ipbc % nxi - P.npbc[0], iy = (ipbc / nxi) % nyi - P.npbc[1], iz = ipbc / (nxi * nyi) - P.npbc[2];
+        const int kI = L.nimg - 1 - k;
+        const unsigned short* Il = at<unsigned short>(L.clist) + kI * L.maxNA;
+        const unsigned short* Jl = at<unsigned short>(L.clist) + k * L.maxNA;
+        const int nI = at<int>(L.ccnt)[kI], nJ = at<int>(L.ccnt)[k];
+        const int ci = 32 * ti + lane;
+        const bool vi = ci < nI;
+        const int i = vi ? (int)Il[ci] : 0;
+        const float3 sh = image_shift(lv, ix, iy, iz);
+        float4 pi = spos[i];
+        pi.x -= sh.x; pi.y -= sh.y; pi.z -= sh.z;
+        const float4 Ri = sREQ[i];
+        // excluded j-slots of this tile
+        const int j0 = 32 * tj;
+        uint32_t xm = ~0u;
+        if (vi) {
+            const int nvalid = nJ - j0;
+            xm = nvalid >= 32 ? 0u : ~((1u << nvalid) - 1u);
+            const int4 ng = ngs(i), ngC = ngc(i);
+            const int e[5] = {i, ngC.x == ipbc ? ng.x : -1, ngC.y == ipbc ? ng.y : -1, ngC.z == ipbc ? ng.z : -1,
+                              ngC.w == ipbc ? ng.w : -1};
+#pragma unroll
+            for (int q = 0; q < 5; q++) {
+                const int d = cand_slot(k, e[q]) - j0;
+                if (d >= 0 && d < 32) xm |= 1u << d;
+            }
+        }
+        float3 fi = make_float3(0.f, 0.f, 0.f), rj = make_float3(0.f, 0.f, 0.f);
+        bool ok;
+        float e = 0.f;
+        const int jlast = nJ - 1;
+#pragma unroll kTileUnroll
+        for (int s = 0; s < 32; s++) {
+            const int jl = (lane + s) & 31;
+            const int j = Jl[min(j0 + jl, jlast)];
+            const float4 pj = spos[j], Rj = sREQ[j];
+            const bool excl = (xm >> jl) & 1u;
+            const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+            const float F = pair_force<ENERGY, HB>(dx, dy, dz, Ri, Rj, excl, Rc2, kq, rc, CUT, ok, e);
+            fi.x = fmaf(dx, F, fi.x); fi.y = fmaf(dy, F, fi.y); fi.z = fmaf(dz, F, fi.z);
+            rj.x = fmaf(-dx, F, rj.x); rj.y = fmaf(-dy, F, rj.y); rj.z = fmaf(-dz, F, rj.z);
+            if (ENERGY) ec += e;
+            if (COUNT && ok) npair += 2;
+            const int nxt = (lane + 1) & 31;
+            rj.x = __shfl_sync(0xffffffffu, rj.x, nxt);
+            rj.y = __shfl_sync(0xffffffffu, rj.y, nxt);
+            rj.z = __shfl_sync(0xffffffffu, rj.z, nxt);
+        }
+        if (vi) fix_add(facc + 3 * i, fi);
+        if (j0 + lane < nJ) fix_add(facc + 3 * (int)Jl[j0 + lane], rj);
+    }
+
+    // mirror pair (k, nimg-1-k): tiles (true) or ordered rows of both images.
+    // Cost in pair evaluations: a tile evaluates 32 x 32 pairs at ~1.2 times
+    // the cost of an ordered pair (the reaction and its rotation); the rows
+    // evaluate the nI x nJ pairs of each image.
+    __device__ __forceinline__ bool image_tiled(int nI, int nJ, int& units) const {
+        const int nti = (nI + 31) >> 5, ntj = (nJ + 31) >> 5;
+        if (kImgTiles && 6 * 1024 * nti * ntj <= 5 * 2 * nI * nJ) { units = nti * ntj; return true; }
+        units = 0;
+        return false;
+    }
+
+    // LISTS: the candidate lists of this step exist (block-uniform; the
+    // central-only form keeps the image code out of the tile loop).
+    // Warp units: each off-diagonal tile and pairs of diagonal tiles of the
+    // central image, then the tiles of the mirror pairs with long candidate
+    // lists; all of equal cost (1024 pair evaluations), dealt round-robin to
+    // the warps.  Then, thread units: the mirror pairs with short lists as
+    // ordered rows of both images, S lanes per candidate atom i (the images
+    // that reach a few edge atoms of a small molecule).  No barrier anywhere:
+    // every sum goes to the fixed-point accumulators.
+    template <bool HB, bool LISTS>
+    __device__ void pair_tiles(const float4* spos, const float4* sREQ, bool pbc, int central, long long* facc,
+                               float& ec) {
         const int B = (natoms + 31) >> 5;
         const int noff = B * (B - 1) / 2;
-        const int nunits = noff + ((B + 1) >> 1);
+        const int ncen = noff + ((B + 1) >> 1);
+        int nunits = ncen, nrows = 0;
+        const int* ccnt = at<int>(L.ccnt);
+        if (LISTS)
+            for (int k = 0; k < L.nimg / 2; k++) {
+                int n;
+                if (image_tiled(ccnt[L.nimg - 1 - k], ccnt[k], n)) nunits += n;
+                else nrows += ccnt[L.nimg - 1 - k] + ccnt[k];
+            }
         for (int u = warp; u < nunits; u += L.nwarps) {
             if (u < noff) {
                 int bi = 0, rem = u;
                 while (rem >= B - 1 - bi) { rem -= B - 1 - bi; bi++; }
                 off_tile<HB>(bi, bi + 1 + rem, spos, sREQ, pbc, central, facc, ec);
-            } else {
+            } else if (u < ncen) {
                 const int d = 2 * (u - noff);
                 diag_tile<HB>(d, spos, sREQ, pbc, central, facc, ec);
                 if (d + 1 < B) diag_tile<HB>(d + 1, spos, sREQ, pbc, central, facc, ec);
+            } else if (LISTS && kImgTiles) {
+                int rem = u - ncen, k = 0, n = 0;
+                for (;; k++) {
+                    if (image_tiled(ccnt[L.nimg - 1 - k], ccnt[k], n) && rem < n) break;
+                    rem -= n;
+                }
+                const int ntj = (ccnt[k] + 31) >> 5;
+                image_tile<HB>(k, rem / ntj, rem % ntj, spos, sREQ, facc, ec);
+            }
+        }
+        if (LISTS && nrows > 0) {
+            const int nxi = 2 * P.npbc[0] + 1, nyi = 2 * P.npbc[1] + 1;
+            const unsigned short* clist = at<unsigned short>(L.clist);
+            for (int u0 = 0; u0 < nrows * S; u0 += T) {
+                const int u = u0 + tid;
+                int c = u / S;
+                const int sub = u % S;
+                float fx = 0.f, fy = 0.f, fz = 0.f, ei = 0.f;
+                int i = -1;
+                if (c < nrows) {
+                    // row c -> image kk (k, then its mirror) and candidate position
+                    int kk = -1;
+                    for (int k = 0; k < L.nimg / 2; k++) {
+                        int n;
+                        if (image_tiled(ccnt[L.nimg - 1 - k], ccnt[k], n)) continue;
+                        const int nI = ccnt[L.nimg - 1 - k], nJ = ccnt[k];
+                        if (c < nI) { kk = k; break; }
+                        c -= nI;
+                        if (c < nJ) { kk = L.nimg - 1 - k; break; }
+                        c -= nJ;
+                    }
+                    const int ipbc = kk < L.nimg / 2 ? kk : kk + 1;
+                    const int ix = ipbc % nxi - P.npbc[0], iy = (ipbc / nxi) % nyi - P.npbc[1];
+                    const int iz = ipbc / (nxi * nyi) - P.npbc[2];
+                    i = clist[(L.nimg - 1 - kk) * L.maxNA + c];
+                    pair_image_row(spos, sREQ, i, sub, spos[i], sREQ[i], ngs(i), ngc(i), pbc, ipbc, ix, iy, iz,
+                                   clist + kk * L.maxNA, ccnt[kk], fx, fy, fz, ei);
+                }
+#pragma unroll
+                for (int o = S / 2; o > 0; o >>= 1) {
+                    fx += __shfl_xor_sync(0xffffffffu, fx, o);
+                    fy += __shfl_xor_sync(0xffffffffu, fy, o);
+                    fz += __shfl_xor_sync(0xffffffffu, fz, o);
+                }
+                if (i >= 0 && sub == 0) fix_add(facc + 3 * i, make_float3(fx, fy, fz));
+                if (ENERGY) ec += 0.5f * ei;
             }
         }
     }
@@ -414,7 +582,6 @@ struct Engine {
             for (int a = t0; a < natoms; a += nt) fgr[a] = make_float4(0, 0, 0, 0);
             return;
         }
-        const float4* sPLQ = at<float4>(L.PLQ);
         const int nunits = natoms * 4;
         for (int u0 = 0; u0 < nunits; u0 += nt) {
             const int u = u0 + t0;
@@ -424,7 +591,7 @@ struct Engine {
                 const float4 p = spos[i];
                 const float3 uu = make_float3((p.x + gorg.x) * P.ginv[0], (p.y + gorg.y) * P.ginv[1],
                                               (p.z + gorg.z) * P.ginv[2]);
-                r = grid_slice(P.grid, P.gn[0], P.gn[1], P.gn[2], uu, sPLQ[i], a);
+                r = grid_slice(P.grid, P.gn[0], P.gn[1], P.gn[2], uu, plq(i), a);
             }
 #pragma unroll
             for (int o = 2; o > 0; o >>= 1) {
@@ -464,8 +631,6 @@ struct Engine {
         float4* fnb = at<float4>(L.fnb);
         float4* fgr = at<float4>(L.fgrid);
         const float4* sREQ = at<float4>(L.REQ);
-        const int4* sng = at<int4>(L.ng);
-        const int4* sngC = at<int4>(L.ngC);
         float4* fng = at<float4>(L.fng);
         // Bonded terms and the GridFF stencil are independent: when the nodes
         // fill only part of the block, the other warps sample the grid at the
@@ -480,9 +645,9 @@ struct Engine {
         for (int ia = tid; ia < natoms; ia += Tb) {
             if (ia >= nnode) { fasm[ia] = make_float4(0, 0, 0, 0); continue; }
             BondedOut o;
-            eval_atom<ENERGY>(ia, natoms, nnode, flags, P.Fmax2NB, spos, sREQ, sng[ia], sngC[ia],
-                              at<float4>(L.apar)[ia], at<float4>(L.bL)[ia], at<float4>(L.bK)[ia],
-                              at<float4>(L.ksp)[ia], at<float4>(L.kpp)[ia], lv, P.npbc[0], P.npbc[1], P.npbc[2], o);
+            eval_atom<ENERGY>(ia, natoms, nnode, flags, P.Fmax2NB, spos, sREQ, ngs(ia), ngc(ia),
+                              npar(L.apar, Y.apars, ia), npar(L.bL, Y.bLs, ia), npar(L.bK, Y.bKs, ia),
+                              npar(L.ksp, Y.Ksp, ia), npar(L.kpp, Y.Kpp, ia), lv, P.npbc[0], P.npbc[1], P.npbc[2], o);
             fasm[ia] = make_float4(o.fa.x, o.fa.y, o.fa.z, 0.f);
             fasm[natoms + ia] = make_float4(o.fpi.x, o.fpi.y, o.fpi.z, 0.f);
 #pragma unroll
@@ -507,16 +672,20 @@ struct Engine {
             const bool lists = L.nimg > 0 && any_shift;
             if (lists) build_candidates();
             const int central = (npz * nyi + npy) * nxi + npx;
-            const unsigned short* clist = at<unsigned short>(L.clist);
-            const int* ccnt = at<int>(L.ccnt);
-            // central image: every unordered pair once, into fixed-point sums
+            // central image and (with candidate lists) the shifted images:
+            // every unordered pair once or ordered rows, into fixed-point sums
             long long* facc = at<long long>(L.facc);
             for (int a = tid; a < 3 * natoms; a += T) facc[a] = 0;
             __syncthreads();
             {
                 float ec = 0.f;
-                if (hasH) central_tiles<true>(spos, sREQ, pbc, central, facc, ec);
-                else central_tiles<false>(spos, sREQ, pbc, central, facc, ec);
+                if (hasH) {
+                    if (lists) pair_tiles<true, true>(spos, sREQ, pbc, central, facc, ec);
+                    else pair_tiles<true, false>(spos, sREQ, pbc, central, facc, ec);
+                } else {
+                    if (lists) pair_tiles<false, true>(spos, sREQ, pbc, central, facc, ec);
+                    else pair_tiles<false, false>(spos, sREQ, pbc, central, facc, ec);
+                }
                 if (ENERGY) Enb += (double)ec;
             }
             __syncthreads();
@@ -536,7 +705,7 @@ struct Engine {
                     if (i < natoms) {
                         const float4 pi = spos[i];
                         const float4 Ri = sREQ[i];
-                        const int4 ng = sng[i], ngC = sngC[i];
+                        const int4 ng = ngs(i), ngC = ngc(i);
                         for (int iz = -npz; iz <= npz; iz++)
                             for (int iy = -npy; iy <= npy; iy++)
                                 for (int ix = -npx; ix <= npx; ix++) {
@@ -559,48 +728,6 @@ struct Engine {
                     }
                     if (ENERGY) Enb += 0.5 * e;
                 }
-            }
-            // pass 2: each shifted image, its candidate atoms j against the
-            // candidate atoms i of the opposite image (the atoms within the
-            // cutoff of this image's box); one image at a time, so every i
-            // is updated by one thread between barriers
-            if (lists) {
-                int kimg = 0;
-                for (int iz = -npz; iz <= npz; iz++)
-                    for (int iy = -npy; iy <= npy; iy++)
-                        for (int ix = -npx; ix <= npx; ix++) {
-                            const int ipbc = ((iz + npz) * nyi + (iy + npy)) * nxi + (ix + npx);
-                            if (ipbc == central) continue;
-                            const int k = kimg++;
-                            if (!image_active(ix, iy, iz)) continue;
-                            const int nI = ccnt[L.nimg - 1 - k], nJ = ccnt[k];
-                            if (nI == 0 || nJ == 0) continue;
-                            const unsigned short* Il = clist + (L.nimg - 1 - k) * L.maxNA;
-                            const unsigned short* Jl = clist + k * L.maxNA;
-                            __syncthreads();
-                            for (int u0 = 0; u0 < nI * S; u0 += T) {
-                                const int u = u0 + tid;
-                                const int c = u / S, sub = u % S;
-                                float fx = 0.f, fy = 0.f, fz = 0.f, ei = 0.f;
-                                int i = -1;
-                                if (c < nI) {
-                                    i = Il[c];
-                                    pair_image_row(spos, sREQ, i, sub, spos[i], sREQ[i], sng[i], sngC[i], pbc, ipbc, ix, iy, iz,
-                                                   Jl, nJ, fx, fy, fz, ei);
-                                }
-#pragma unroll
-                                for (int o = S / 2; o > 0; o >>= 1) {
-                                    fx += __shfl_xor_sync(0xffffffffu, fx, o);
-                                    fy += __shfl_xor_sync(0xffffffffu, fy, o);
-                                    fz += __shfl_xor_sync(0xffffffffu, fz, o);
-                                }
-                                if (i >= 0 && sub == 0) {
-                                    const float4 a = fnb[i];
-                                    fnb[i] = make_float4(a.x + fx, a.y + fy, a.z + fz, 0.f);
-                                }
-                                if (ENERGY) Enb += 0.5 * (double)ei;
-                            }
-                        }
             }
         } else {
             for (int a = tid; a < natoms; a += T) fnb[a] = make_float4(0, 0, 0, 0);
@@ -627,7 +754,6 @@ struct Engine {
         float4* fasm = at<float4>(L.fasm);
         const float4* fnb = at<float4>(L.fnb);
         const float4* fgr = at<float4>(L.fgrid);
-        const int4* sbk = at<int4>(L.bk);
         const float4* fng = at<float4>(L.fng);
         const float4* spos = at<float4>(L.pos);
         const float4* svel = at<float4>(L.vel);
@@ -637,7 +763,7 @@ struct Engine {
             if (v < natoms) {
                 const float4 a = fasm[v], b = fnb[v], c = fgr[v];
                 f = make_float3(a.x + b.x + c.x, a.y + b.y + c.y, a.z + b.z + c.z);
-                const int4 bk = sbk[v];
+                const int4 bk = bks(v);
                 const int bks[4] = {bk.x, bk.y, bk.z, bk.w};
 #pragma unroll
                 for (int k = 0; k < 4; k++) {
@@ -647,7 +773,7 @@ struct Engine {
             } else {
                 const int ia = v - natoms;
                 f = f3(fasm[v]);
-                const int4 bk = sbk[ia];
+                const int4 bk = bks(ia);
                 const int bks[4] = {bk.x, bk.y, bk.z, bk.w};
 #pragma unroll
                 for (int k = 0; k < 4; k++) {
