@@ -158,7 +158,11 @@ def run_ours(args):
     natoms = batch.natoms.astype(np.int64)
     # launch shapes from the autotuner (untimed; the choice is reported)
     t0 = time.perf_counter()
-    tune_rows = w.autotune(nstep_probe=50) if not args.no_tune else []
+    tune_rows = []
+    if args.tuning and w.load_tuning(args.tuning):
+        pass                                    # saved launch shapes of an earlier run
+    elif not args.no_tune:
+        tune_rows = w.autotune(nstep_probe=50, path=args.tuning)
     tune_s = time.perf_counter() - t0
     w.set_graph(True)
     # counting pass (untimed): algorithmic work of one relaxation of this batch
@@ -603,6 +607,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner (heuristic shapes)")
+    ap.add_argument("--tuning", default=None,
+                    help="JSON file of launch shapes: loaded if it exists, else written by the autotuner")
     ap.add_argument("--maxsteps", type=int, default=MAXSTEPS, help="FIRE step limit per system (profiling runs use fewer)")
     args = ap.parse_args()
     MAXSTEPS = args.maxsteps
