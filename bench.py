@@ -373,23 +373,47 @@ def parity_subset(w, batch, sub, C, nsub=64):
             "reference": "FP64 oracle (restatement pinned to FireCore's compiled run_no_omp physics)"}
 
 
-def geometry_parity(batch, st0, r, nsample):
+def geometry_parity(batch, st0, r, nsample, P, F, C, ncores):
     """Relaxed geometries of the device (st0) against the oracle's FP64
     relaxation of the same first nsample systems (r): atom RMSD per system
-    converged in both."""
+    converged in both.  At Fmax < 1e-4 eV/A a soft mode (a molecule sliding on
+    the slab, k ~ 0.01 eV/A^2) leaves ~0.01 A of slack, so FP32 and FP64
+    trajectories stop at different points of the same basin; both end points
+    are therefore also re-relaxed in FP64 to Fmax < 1e-6 eV/A (untimed) and
+    compared again: agreement there means the same minimum."""
+    from oracle import oracle as O
     _, _, v = batch.offsets()
     both = [s for s in range(nsample) if st0["status"][s] == 1 and r["converged"][s] == 1]
+    if not both:
+        return {"systems_converged_in_both": 0}
+    sb = batch.subset(both)
+    _, _, vb = sb.offsets()
+    rows = np.concatenate([np.arange(v[s], v[s + 1]) for s in both])
     _, _, vs = batch.subset(range(nsample)).offsets()
-    rmsd = []
-    for s in both:
-        na = int(batch.natoms[s])
-        d = st0["pos"][v[s]:v[s] + na, :3] - r["pos"][vs[s]:vs[s] + na, :3]
-        rmsd.append(float(np.sqrt((d ** 2).sum(1).mean())))
-    rmsd = np.array(rmsd)
+    rows_r = np.concatenate([np.arange(vs[s], vs[s + 1]) for s in both])
+
+    def rmsd(pa, pb):
+        out = []
+        for k in range(len(both)):
+            na = int(sb.natoms[k])
+            d = pa[vb[k]:vb[k] + na, :3] - pb[vb[k]:vb[k] + na, :3]
+            out.append(float(np.sqrt((d ** 2).sum(1).mean())))
+        return np.array(out)
+
+    pd, po = st0["pos"][rows], r["pos"][rows_r]
+    r0 = rmsd(pd, po)
+    td = O.relax(sb, P, F, C, niter=30000, Fconv=1e-6, conv_mode=1, pos=pd, nthreads=ncores)
+    to = O.relax(sb, P, F, C, niter=30000, Fconv=1e-6, conv_mode=1, pos=po, nthreads=ncores)
+    ok = (td["converged"] == 1) & (to["converged"] == 1)
+    r1 = rmsd(td["pos"], to["pos"])[ok]
     return {"systems_converged_in_both": len(both),
-            "fraction_rmsd_le_1e-3_A": float((rmsd <= 1e-3).mean()) if len(rmsd) else None,
-            "median_rmsd_A": float(np.median(rmsd)) if len(rmsd) else None,
-            "max_rmsd_A": float(rmsd.max()) if len(rmsd) else None}
+            "fraction_rmsd_le_1e-3_A": float((r0 <= 1e-3).mean()),
+            "median_rmsd_A": float(np.median(r0)), "max_rmsd_A": float(r0.max()),
+            "same_minimum": {"method": "both end points re-relaxed by the FP64 oracle to Fmax < 1e-6 eV/A",
+                             "systems": int(ok.sum()),
+                             "fraction_rmsd_le_1e-3_A": float((r1 <= 1e-3).mean()) if len(r1) else None,
+                             "median_rmsd_A": float(np.median(r1)) if len(r1) else None,
+                             "max_rmsd_A": float(r1.max()) if len(r1) else None}}
 
 
 def cpu_baseline(batch, sub, C, args, st0):
@@ -410,7 +434,7 @@ def cpu_baseline(batch, sub, C, args, st0):
     conv = int((r["converged"] == 1).sum())
     return {"value": conv / dt, "unit": UNIT, "cores": ncores, "kind": "port",
             "sample": f"{nsample} of the systems, full relaxation each ({conv} converged, {dt:.1f} s), CPU: {model}",
-            "geometry": geometry_parity(batch, st0, r, nsample)}
+            "geometry": geometry_parity(batch, st0, r, nsample, P, F, C, ncores)}
 
 
 # --------------------------------------------------------------------------- learned vs plain
