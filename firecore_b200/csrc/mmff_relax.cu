@@ -591,7 +591,7 @@ struct Engine {
                 const float4 p = spos[i];
                 const float3 uu = make_float3((p.x + gorg.x) * P.ginv[0], (p.y + gorg.y) * P.ginv[1],
                                               (p.z + gorg.z) * P.ginv[2]);
-                r = grid_slice(P.grid, P.gn[0], P.gn[1], P.gn[2], uu, plq(i), a);
+                r = grid_slice<(T >= 128) ? 4 : 1>(P.grid, P.gn[0], P.gn[1], P.gn[2], uu, plq(i), a);
             }
 #pragma unroll
             for (int o = 2; o > 0; o >>= 1) {
