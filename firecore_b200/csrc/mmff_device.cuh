@@ -374,9 +374,9 @@ __device__ __forceinline__ float comp(float4 v, int k) { return k == 0 ? v.x : (
 // grid coordinate u (already in voxel units).  Returns the slice's partial
 // (dE/dx*bx', E-channel combos) as (Fx, Fy, Fz, E) *before* the -1/step scale.
 // UNROLL: y-columns of the slice unrolled (their 16 loads in flight together).
-// In the fused relax step of 64-thread blocks (eight per SM) the step's code,
-// not its loads, is the limit: there no unrolling measured 5-7 % faster; the
-// larger blocks keep all four (5 % faster there).
+// In the fused relax step of small blocks (four or eight per SM) the step's
+// code, not its loads, is the limit: there no unrolling measured 5-7 % faster;
+// the 256-thread blocks keep all four (5 % faster there).
 template <int UNROLL = 4>
 __device__ __forceinline__ float4 grid_slice(const float4* __restrict__ G, int nx, int ny, int nz, float3 u,
                                              float4 PLQ, int a) {

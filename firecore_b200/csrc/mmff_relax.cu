@@ -18,6 +18,14 @@
 #include "mmff_device.cuh"
 #include <cfloat>
 
+// blocks of at least this many threads unroll the pair tiles and the GridFF
+// columns; smaller ones (four or eight per SM, instruction-fetch bound) do
+// not: measured +5-7 % at 64 threads, +1.7 % at 128 threads (C2 class of
+// 65-128 atoms), while the 256-thread blocks gain 5 % from unrolling
+#ifndef MMFF_UNROLL_MIN_T
+#define MMFF_UNROLL_MIN_T 256
+#endif
+
 namespace mmff {
 
 // warp-level sums / extrema
@@ -301,10 +309,11 @@ struct Engine {
 #ifndef MMFF_TILE_UNROLL_LARGE
 #define MMFF_TILE_UNROLL_LARGE 4
 #endif
-    // tile-step unrolling (build options): none in 64-thread blocks, whose
-    // fused step is instruction-fetch bound at eight blocks per SM (unrolling
-    // by 4 measured -6 % there), 4 in the larger blocks (+4 %)
-    static constexpr int kTileUnroll = T >= 128 ? MMFF_TILE_UNROLL_LARGE : MMFF_TILE_UNROLL_SMALL;
+    // tile-step unrolling (build options): none in blocks below
+    // MMFF_UNROLL_MIN_T threads, whose fused step is instruction-fetch bound
+    // (unrolling by 4 measured -6 % at 64 threads), 4 in the larger blocks
+    // (+4.7 %)
+    static constexpr int kTileUnroll = T >= MMFF_UNROLL_MIN_T ? MMFF_TILE_UNROLL_LARGE : MMFF_TILE_UNROLL_SMALL;
     __device__ __forceinline__ void fix_add(long long* a, float3 f) {
         atomicAdd(reinterpret_cast<unsigned long long*>(a + 0), (unsigned long long)__float2ll_rn(f.x * kFix));
         atomicAdd(reinterpret_cast<unsigned long long*>(a + 1), (unsigned long long)__float2ll_rn(f.y * kFix));
@@ -597,7 +606,7 @@ struct Engine {
                 const float4 p = spos[i];
                 const float3 uu = make_float3((p.x + gorg.x) * P.ginv[0], (p.y + gorg.y) * P.ginv[1],
                                               (p.z + gorg.z) * P.ginv[2]);
-                r = grid_slice<(T >= 128) ? 4 : 1>(P.grid, P.gn[0], P.gn[1], P.gn[2], uu, plq(i), a);
+                r = grid_slice<(T >= MMFF_UNROLL_MIN_T) ? 4 : 1>(P.grid, P.gn[0], P.gn[1], P.gn[2], uu, plq(i), a);
             }
 #pragma unroll
             for (int o = 2; o > 0; o >>= 1) {
