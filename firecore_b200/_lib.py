@@ -8,7 +8,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("MMFF_LIB", os.path.join(HERE, "libMMFFmulti_lib.so"))
+GEN_PATH = os.path.join(HERE, "libmmff_gen.so")
 _lib = None
+_gen = None
 
 
 def load() -> ctypes.CDLL:
@@ -23,6 +25,30 @@ def load() -> ctypes.CDLL:
     return _lib
 
 
+def gen() -> ctypes.CDLL:
+    """Load the host-only workload generator (``libmmff_gen.so``: the seeded
+    molecules and slabs of ``csrc/molgen.cpp``, no CUDA)."""
+    global _gen
+    if _gen is None:
+        if not os.path.exists(GEN_PATH):
+            raise RuntimeError(f"{GEN_PATH} is missing: run `python -m firecore_b200.build` first")
+        g = ctypes.CDLL(GEN_PATH, mode=ctypes.RTLD_LOCAL)
+        _declare_gen(g)
+        _gen = g
+    return _gen
+
+
+def _declare_gen(lib):
+    c_int, c_double, c_void = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
+    lib.mmff_gen_nnode.argtypes = [c_int]
+    lib.mmff_gen_nnode.restype = c_int
+    lib.mmff_gen_systems.argtypes = [c_int, c_void, ctypes.c_uint64, c_int, c_double, c_int, c_double, c_void,
+                                     c_int] + [c_void] * 11 + [c_int]
+    lib.mmff_gen_systems.restype = c_int
+    lib.mmff_gen_slab.argtypes = [c_double, c_int, c_int, c_double, c_double, c_void, c_void, c_void, c_void]
+    lib.mmff_gen_slab.restype = c_int
+
+
 def ptr(a):
     """ctypes void pointer to a numpy array or torch tensor (None -> NULL)."""
     if a is None:
@@ -35,13 +61,7 @@ def ptr(a):
 
 def _declare(lib):
     c_int, c_double, c_void = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
-    lib.mmff_gen_nnode.argtypes = [c_int]
-    lib.mmff_gen_nnode.restype = c_int
-    lib.mmff_gen_systems.argtypes = [c_int, c_void, ctypes.c_uint64, c_int, c_double, c_int, c_double, c_void,
-                                     c_int] + [c_void] * 11 + [c_int]
-    lib.mmff_gen_systems.restype = c_int
-    lib.mmff_gen_slab.argtypes = [c_double, c_int, c_int, c_double, c_double, c_void, c_void, c_void, c_void]
-    lib.mmff_gen_slab.restype = c_int
+    _declare_gen(lib)
     lib.mmff_last_error.argtypes = []
     lib.mmff_last_error.restype = ctypes.c_char_p
     sig = {
@@ -70,6 +90,8 @@ def _declare(lib):
         f = getattr(lib, name)
         f.argtypes = args
         f.restype = c_int
+    lib.mmff_kernel_launches.argtypes = []
+    lib.mmff_kernel_launches.restype = ctypes.c_ulonglong
     lib.mmff_timer_stop.argtypes = []
     lib.mmff_timer_stop.restype = c_double
     lib.mmff_peak_fp32.argtypes = []

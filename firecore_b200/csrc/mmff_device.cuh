@@ -26,7 +26,17 @@ enum : int {
     F_BONDS = 1 << 0, F_PIPI = 1 << 1, F_PISIGMA = 1 << 2, F_ANGLES = 1 << 3,
     F_SUB_ANGLE_NB = 1 << 4, F_SUB_BOND_NB = 1 << 5, F_CLAMP_NB = 1 << 6,
     F_NONBONDED = 1 << 7, F_GRID = 1 << 8, F_PBC = 1 << 9, F_SURF = 1 << 10,
+    // set by the host (never by callers): the 1-3 pairs of the angle terms
+    // are left out of the central-image pair sum instead of being added there
+    // and subtracted again in the angle term (see pair13)
+    F_EXCL13 = 1 << 11,
 };
+
+// The host turns F_EXCL13 on exactly when the angle terms subtract the 1-3
+// pair term that the pair sum adds and nothing clamps the pair forces.
+__host__ __device__ inline bool excl13_active(int flags) {
+    return (flags & F_SUB_ANGLE_NB) && (flags & F_ANGLES) && (flags & F_NONBONDED) && !(flags & F_CLAMP_NB);
+}
 
 // status codes per system
 enum : int { ST_RUNNING = 0, ST_CONVERGED = 1, ST_MAXSTEPS = 2, ST_NAN = -1 };
@@ -96,6 +106,9 @@ struct Systems {
     const float4* __restrict__ bKs;
     const float4* __restrict__ Ksp;
     const float4* __restrict__ Kpp;
+    const int* __restrict__ a13;        // per node: angle pairs (bit t of slots i<j) whose 1-3 pair the pair sum skips
+    const uint32_t* __restrict__ xmask; // central-image exclusion words: row (atom i) of ceil(natoms/32) words per system
+    const int* __restrict__ moff;       // per system: first word of its exclusion rows
     float4* pos;                        // local frame
     float4* vel;
     float4* force;                      // assembled forces (written by eval / at exit)
@@ -144,6 +157,36 @@ __device__ __forceinline__ float ljqh(float r2, float R0, float E0, float Q, flo
     const float H = u6 * vdW * hw;              // u6*u6*(w<0 ? w*E0 : 0)
     if (ENERGY) E = fmaf(u6 - 2.f, vdW, Eel + H);
     return -fmaf(12.f * ir2, fmaf(u6 - 1.f, vdW, H), Eel * ir2);
+}
+
+// 1-3 pair (ends of an angle) of the angle term, MMFFsp3_loc.h:525-538.  The
+// reference adds this pair in the pair sum and subtracts getLJQH of it here;
+// both are ~10^2-10^3 eV/A for close 1-3 contacts, so in FP32 the difference
+// keeps the rounding of the large terms.  With x13 the pair sum skipped the
+// pair (central image), and this adds what the pair term has beyond getLJQH:
+// the shifted-force Coulomb part inside the cutoff (zero without one), or
+// -getLJQH beyond it.  Either way the total equals the reference's sum in
+// exact arithmetic.  Returns the scalar F of the force on the first atom
+// (dp * F, dp = p_second - p_first); e: energy change, ep (x13 only): the
+// pair energy the pair sum would have counted (for the energy split).
+template <bool ENERGY>
+__device__ __forceinline__ float pair13(float r2, float4 Ri, float4 Rj, bool x13, float Rc2, float kq, float rc,
+                                        float& e, float& ep) {
+    const float R0 = Ri.x + Rj.x, E0 = Ri.y * Rj.y, Q = Ri.z * Rj.z, hw = fminf(Ri.w * Rj.w, 0.f);
+    if (x13 && r2 < Rc2) {
+        const float ir = rsqrtf(r2);
+        if (ENERGY) {
+            float eL;
+            ljqh<true>(r2, R0, E0, Q, hw, eL);
+            e = Q * kq * (r2 * ir - 2.f * rc);
+            ep = eL + e;
+        }
+        return Q * kq * ir;
+    }
+    float eL = 0.f;
+    const float F = ljqh<ENERGY>(r2, R0, E0, Q, hw, eL);
+    if (ENERGY) { e = -eL; ep = 0.f; }
+    return -F;
 }
 
 // scalar pair force F (f_i += d F with d = p_j - p_i) of one pair-image, the
@@ -217,20 +260,36 @@ struct BondedOut {
     float3 fa, fpi;
     float3 fbs[4], fps[4];
     float E;
+    float E13;      // ENERGY: pair energies of the 1-3 pairs the pair sum skipped
 };
+
+// cutoff constants of the pair term as the 1-3 residual needs them
+struct Cut13 {
+    float Rc2, kq, rc;
+    __device__ __forceinline__ Cut13(const Params& P) {
+        const bool cut = P.Rc2 > 0.f;
+        Rc2 = cut ? P.Rc2 : 3.0e38f;
+        kq = P.kq_rc2;
+        rc = cut ? sqrtf(1.f / kq) : 0.f;
+    }
+};
+
+// angle pair index of neighbour slots i < j (0..5): (0,1) (0,2) (0,3) (1,2) (1,3) (2,3)
+__host__ __device__ constexpr int angle_slot(int i, int j) { return i * (7 - i) / 2 + (j - i - 1); }
 
 template <bool ENERGY>
 __device__ __forceinline__ void eval_atom(int ia, int natoms, int nnode, int flags, float Fmax2,
                                           const float4* sp, const float4* sREQ, int4 ng, int4 ngC,
                                           float4 apar, float4 bL, float4 bK, float4 ksp, float4 kpp,
-                                          const float* lv, int npx, int npy, int npz, BondedOut& o) {
+                                          const float* lv, int npx, int npy, int npz, int a13, const Cut13& cu,
+                                          BondedOut& o) {
     const float3 pa = f3(sp[ia]);
     const float3 hpi = f3(sp[natoms + ia]);
     float3 fa = make_float3(0, 0, 0), fpi = make_float3(0, 0, 0);
     float3 fbs[4], fps[4];
     float3 hf[4];
     float he[4], hl[4];
-    float E = 0.f;
+    float E = 0.f, E13 = 0.f;
     const int ings[4] = {ng.x, ng.y, ng.z, ng.w};
     const int ingC[4] = {ngC.x, ngC.y, ngC.z, ngC.w};
     const float bLa[4] = {bL.x, bL.y, bL.z, bL.w};
@@ -336,16 +395,17 @@ __device__ __forceinline__ void eval_atom(int ia, int natoms, int nnode, int fla
                 fa = fa - (f1 + f2);
                 if (flags & F_SUB_ANGLE_NB) {
                     const int ing = ings[i], jng = ings[j];
-                    const float4 Ri = sREQ[ing], Rj = sREQ[jng];
-                    const float hw = fminf(Ri.w * Rj.w, 0.f);
                     const float3 dp = hf[j] * hl[j] - hf[i] * hl[i];
-                    float e;
-                    const float F = ljqh<ENERGY>(dot3(dp, dp), Ri.x + Rj.x, Ri.y * Rj.y, Ri.z * Rj.z, hw, e);
+                    // x13: the pair sum skipped this central-image pair
+                    const bool x13 = (flags & F_EXCL13) && ((a13 >> angle_slot(i, j)) & 1) &&
+                                     (!(flags & F_PBC) || ingC[i] == ingC[j]);
+                    float e = 0.f, ep = 0.f;
+                    const float F = pair13<ENERGY>(dot3(dp, dp), sREQ[ing], sREQ[jng], x13, cu.Rc2, cu.kq, cu.rc, e, ep);
                     float3 fij = dp * F;
                     if (flags & F_CLAMP_NB) { float ff = dot3(fij, fij); if (ff > Fmax2) fij = fij * sqrtf(Fmax2 / ff); }
-                    if (ENERGY) E -= e;
-                    f1 = f1 - fij;
-                    f2 = f2 + fij;
+                    if (ENERGY) { E += e; E13 += ep; }
+                    f1 = f1 + fij;
+                    f2 = f2 - fij;
                 }
                 fbs[i] = fbs[i] + f1;
                 fbs[j] = fbs[j] + f2;
@@ -356,6 +416,7 @@ __device__ __forceinline__ void eval_atom(int ia, int natoms, int nnode, int fla
 #pragma unroll
     for (int i = 0; i < 4; i++) { o.fbs[i] = fbs[i]; o.fps[i] = fps[i]; }
     o.E = E;
+    o.E13 = E13;
 }
 
 // ----- cubic B-spline basis (Bspline.h:254, :267)

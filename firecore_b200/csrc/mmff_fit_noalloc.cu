@@ -22,14 +22,11 @@
 #include "mmff_host.h"
 
 #define MMFF_FIT_NMAX 4096
-#define MMFF_FIT_MAXDEV 64
 
 // per axis: cp[NMAX], z[NMAX], then scalars (zden) -- 3 axes
 static __device__ __align__(256) double g_fit_scratch[3 * 3 * MMFF_FIT_NMAX];
 
 namespace {
-
-double* g_scratch_ptr[MMFF_FIT_MAXDEV] = {nullptr};
 
 // cp (and for periodic axes z, zden) of the solve of (c[i-1] + 4c[i] + c[i+1])/6 = v[i]
 __global__ void fit_coef_kernel(double* scr, int nx, int ny, int nz) {
@@ -135,16 +132,21 @@ int mmff_bspline_fit_noalloc(double* d_coefs, int nx, int ny, int nz, void* stre
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return fit_fail("mmff_bspline_fit_noalloc: cudaGetDevice", e);
-    if (dev < 0 || dev >= MMFF_FIT_MAXDEV) return fit_fail("mmff_bspline_fit_noalloc: device index out of range");
-    if (!g_scratch_ptr[dev]) {
-        // one-time set-up on this device (with it current): the host-side name
-        // g_fit_scratch is only a stand-in, the kernels need its device address
-        double* p = nullptr;
-        e = cudaGetSymbolAddress((void**)&p, g_fit_scratch);
-        if (e != cudaSuccess || !p) return fit_fail("mmff_bspline_fit_noalloc: cudaGetSymbolAddress", e);
-        g_scratch_ptr[dev] = p;
-    }
-    double* scr = g_scratch_ptr[dev];
+    // the grid must be device (or managed) memory of the current device: a
+    // host pointer or another GPU's buffer is an argument error here, not a
+    // fault inside the solve kernels (the query allocates nothing)
+    cudaPointerAttributes pa;
+    e = cudaPointerGetAttributes(&pa, d_coefs);
+    if (e != cudaSuccess) { cudaGetLastError(); return fit_fail("mmff_bspline_fit_noalloc: grid pointer not known to CUDA", e); }
+    if ((pa.type != cudaMemoryTypeDevice && pa.type != cudaMemoryTypeManaged) || pa.device != dev)
+        return fit_fail("mmff_bspline_fit_noalloc: grid pointer is not device memory of the current device");
+    // device address of the scratch array on the current device, taken on
+    // every call (it allocates nothing): the host-side name g_fit_scratch is
+    // only a stand-in, and an address kept from an earlier call would be
+    // stale after the program reset or recreated this device's context
+    double* scr = nullptr;
+    e = cudaGetSymbolAddress((void**)&scr, g_fit_scratch);
+    if (e != cudaSuccess || !scr) return fit_fail("mmff_bspline_fit_noalloc: cudaGetSymbolAddress", e);
     cudaStream_t st = (cudaStream_t)stream;
     fit_coef_kernel<<<1, 32, 0, st>>>(scr, nx, ny, nz);
     const long lz = (long)nx * ny, ly = (long)nx * nz, lx = (long)ny * nz;

@@ -5,6 +5,8 @@
 
 // Set the message mmff_last_error() returns (C++ linkage, internal to the library).
 void mmff_set_error(const char* msg);
+// Add n to the library's kernel-launch count (mmff_kernel_launches).
+void mmff_count_launches(int n);
 
 extern "C" {
 

@@ -444,12 +444,14 @@ void* init(int nSys, char* xyz_name, char* surf_name, char* smile_name, bool bMM
     return &L;
 }
 
-// Relax every replica on the GPU (all iParalel modes map to the device path);
-// returns the largest number of steps any replica took (run_ocl_opt's count).
+// Relax every replica on the GPU; returns the largest number of steps any
+// replica took (run_ocl_opt's count).  As in MMFFmulti_lib.cpp:116-132, dt
+// and ialg are not used (the FIRE time steps come from set_opt).  iParalel
+// selects the reference's CPU (-1, 0, 1) or OpenCL (2, 3, 4) drivers there;
+// this library has only the device path, so every value runs it.
 int run(int nstepMax, double dt, double Fconv, int ialg, double* outE, double* outF, int iParalel) {
-    (void)ialg; (void)iParalel;
+    (void)dt; (void)ialg; (void)iParalel;
     if (!L.ready) { set_error("run: init() first"); return -1; }
-    if (dt > 0) { L.fire[0] = dt; if (mmff_set_fire(dt, L.fire[1], L.fire[2], L.fire[3], L.fire[4], L.fire[5], (int)L.fire[6], L.fire[7], L.fire[8], 0)) return -1; }
     if (mmff_relax(nstepMax, Fconv, 0)) { set_error(mmff_last_error()); return -1; }
     std::vector<int> ns(L.nSys);
     std::vector<double> fc(L.nSys);

@@ -631,6 +631,7 @@ int check_err(cudaStream_t st, const char* what) {
 int pack_input(const float* d_feat, int n, int ntile, uint8_t* X, cudaStream_t st) {
     const long nchunk = (long)ntile * TILE * (K0 / 8);
     pack_input_kernel<<<(unsigned)((nchunk + 255) / 256), 256, 0, st>>>(d_feat, n, ntile, N.mean.p, N.istd.p, X);
+    mmff_count_launches(1);
     MCK(cudaGetLastError());
     return 0;
 }
@@ -646,9 +647,12 @@ int run_net(bool train, const uint8_t* X, const float4* T, int ntile, int nrows,
     a.ntile = ntile; a.nrows = nrows; a.inv_batch = inv_batch; a.out_scale = N.out_scale;
     if (train) {
         mlp_kernel<true><<<grid, NET_THREADS, SM_ALLOC, st>>>(a);
+        mmff_count_launches(1);
         reduce_grad_kernel<<<(P_TOTAL + 255) / 256, 256, 0, st>>>(N.gpart.p, N.lpart.p, grid, N.grad.p, N.loss.p);
+        mmff_count_launches(1);
     } else {
         mlp_kernel<false><<<grid, NET_THREADS, SM_ALLOC, st>>>(a);
+        mmff_count_launches(1);
     }
     MCK(cudaGetLastError());
     return 0;
@@ -657,6 +661,7 @@ int run_net(bool train, const uint8_t* X, const float4* T, int ntile, int nrows,
 int adamw(int t, double lr, double wd, cudaStream_t st) {
     adamw_pack_kernel<<<(P_TOTAL + 255) / 256, 256, 0, st>>>(N.prm.p, N.grad.p, N.m.p, N.v.p, t, (float)lr, 0.9f,
                                                              0.999f, 1e-8f, (float)wd, N.Wp.p);
+    mmff_count_launches(1);
     MCK(cudaGetLastError());
     return 0;
 }
@@ -681,6 +686,7 @@ int features_device(const WorldView& V, double z_top) {
     const float zoff = (float)(V.gpos0[2] - z_top);
     descriptor_kernel<<<(V.NA + DESC_WARPS - 1) / DESC_WARPS, DESC_WARPS * 32, 0, V.stream>>>(
         V.P, V.Y, N.atom_sys.p, N.elem.p, V.NA, zoff, N.feat.p, N.err.p);
+    mmff_count_launches(1);
     MCK(cudaGetLastError());
     return 0;
 }
@@ -887,17 +893,21 @@ int mmff_mlp_warmstart(int nsteps, double z_top, int* accepted) {
         if (pack_input(N.feat.p, V.NA, ntile, N.Xs.p, V.stream)) return -1;
         if (run_net(false, N.Xs.p, nullptr, ntile, V.NA, 0.f, N.outs.p, V.stream)) return -1;
         save_kernel<<<ga, 256, 0, V.stream>>>(V.Y, N.atom_sys.p, V.NA, N.save.p);
+        mmff_count_launches(1);
         MCK(cudaMemsetAsync(N.keep.p, 0, V.nsys * sizeof(int), V.stream));
         // step-length search along the proposal: the first length that lowers
         // a system's energy is kept, otherwise the system stays where it was
         for (int t = 0; t < kTrials; t++) {
             apply_kernel<<<ga, 256, 0, V.stream>>>(V.Y, N.atom_sys.p, V.NA, N.outs.p, N.save.p, kAlpha[t], N.keep.p);
+            mmff_count_launches(1);
             MCK(cudaGetLastError());
             if (mmff_eval(1) < 0) return -1;
             gate_sys_kernel<<<gs, 256, 0, V.stream>>>(V.nsys, V.Y.energy, N.E0.p, N.keep.p, N.accepted.p);
+            mmff_count_launches(1);
             MCK(cudaGetLastError());
         }
         revert_kernel<<<ga, 256, 0, V.stream>>>(V.Y, N.atom_sys.p, V.NA, N.keep.p, N.save.p);
+        mmff_count_launches(1);
         MCK(cudaGetLastError());
     }
     if (check_err(V.stream, "mmff_mlp_warmstart")) return -1;

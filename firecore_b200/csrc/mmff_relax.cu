@@ -68,6 +68,10 @@ struct Engine {
     // per-step image culling
     float bbmin[3], bbmax[3];
     bool hasH = false;          // any H-bond pseudo-charge in the system (block-uniform)
+    const uint32_t* xrow;       // central-image exclusion rows (ceil(natoms/32) words per atom)
+    int nbw;                    // words per row
+    bool pairbad = false;       // a non-finite pair force reached the fixed-point sums
+    double e13 = 0.0;           // ENERGY: pair energies of the skipped 1-3 pairs (energy split)
     // pair-images evaluated by this thread (COUNT builds only)
     unsigned long long npair = 0;
 
@@ -95,6 +99,9 @@ struct Engine {
         aoff = d.x; noff = d.y; voff = d.z; natoms = d.w;
         nnode = Y.nnode[s];
         nvecs = natoms + nnode;
+        xrow = Y.xmask + Y.moff[s];
+        nbw = (natoms + 31) >> 5;
+        pairbad = false;
 #pragma unroll
         for (int k = 0; k < 9; k++) lv[k] = Y.lvec[9 * s + k];
         const float4 g = Y.gorg[s];
@@ -314,41 +321,36 @@ struct Engine {
     // (unrolling by 4 measured -6 % at 64 threads), 4 in the larger blocks
     // (+4.7 %)
     static constexpr int kTileUnroll = T >= MMFF_UNROLL_MIN_T ? MMFF_TILE_UNROLL_LARGE : MMFF_TILE_UNROLL_SMALL;
+    // Each add is clamped to |f| <= 2^20 eV/A, so the 64-bit sums (2^31 units
+    // of range per eV/A) cannot wrap for any system that fits a block; a
+    // non-finite force (atoms on top of each other) would convert to an
+    // arbitrary integer, so it marks the system bad instead (assemble).
+    static constexpr float kFixMax = 1048576.f;
     __device__ __forceinline__ void fix_add(long long* a, float3 f) {
-        atomicAdd(reinterpret_cast<unsigned long long*>(a + 0), (unsigned long long)__float2ll_rn(f.x * kFix));
-        atomicAdd(reinterpret_cast<unsigned long long*>(a + 1), (unsigned long long)__float2ll_rn(f.y * kFix));
-        atomicAdd(reinterpret_cast<unsigned long long*>(a + 2), (unsigned long long)__float2ll_rn(f.z * kFix));
+        pairbad |= !isfinite(f.x + f.y + f.z);
+        const float x = fminf(fmaxf(f.x, -kFixMax), kFixMax), y = fminf(fmaxf(f.y, -kFixMax), kFixMax);
+        const float z = fminf(fmaxf(f.z, -kFixMax), kFixMax);
+        atomicAdd(reinterpret_cast<unsigned long long*>(a + 0), (unsigned long long)__float2ll_rn(x * kFix));
+        atomicAdd(reinterpret_cast<unsigned long long*>(a + 1), (unsigned long long)__float2ll_rn(y * kFix));
+        atomicAdd(reinterpret_cast<unsigned long long*>(a + 2), (unsigned long long)__float2ll_rn(z * kFix));
     }
 
-    // own atom i of a tile: position, parameters and its bonded neighbours in
-    // the central cell (the excluded j); invalid slots exclude everything
-    struct TileAtom { float4 p, R; int e1, e2, e3, e4; bool v; };
-    __device__ __forceinline__ TileAtom tile_atom(int i, const float4* spos, const float4* sREQ, bool pbc, int central) {
+    // own atom i of a tile: position and parameters; invalid slots exclude everything
+    struct TileAtom { float4 p, R; int i; bool v; };
+    __device__ __forceinline__ TileAtom tile_atom(int i, const float4* spos, const float4* sREQ) {
         TileAtom t;
         t.v = i < natoms;
-        const int ic = t.v ? i : 0;
-        t.p = spos[ic]; t.R = sREQ[ic];
-        const int4 ng = ngs(ic), ngC = ngc(ic);
-        t.e1 = (ngC.x == central || !pbc) ? ng.x : -1;
-        t.e2 = (ngC.y == central || !pbc) ? ng.y : -1;
-        t.e3 = (ngC.z == central || !pbc) ? ng.z : -1;
-        t.e4 = (ngC.w == central || !pbc) ? ng.w : -1;
+        t.i = t.v ? i : 0;
+        t.p = spos[t.i]; t.R = sREQ[t.i];
         return t;
     }
 
-    // excluded j-slots of block bj for this lane's atom: all if the atom is a
-    // padding slot, padding slots of bj, and the atom's bonded neighbours in bj
+    // excluded j-slots of block bj for this lane's atom (the host-built
+    // exclusion row: the atom itself, its bonded neighbours in the central
+    // cell, the 1-3 pairs the angle terms account for, padding slots of bj);
+    // all if the atom is a padding slot
     __device__ __forceinline__ uint32_t tile_mask(const TileAtom& a, int bj) const {
-        if (!a.v) return ~0u;
-        const int nvalid = natoms - 32 * bj;
-        uint32_t m = nvalid >= 32 ? 0u : ~((1u << nvalid) - 1u);
-        const int e[4] = {a.e1, a.e2, a.e3, a.e4};
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const int d = e[k] - 32 * bj;
-            if (e[k] >= 0 && d >= 0 && d < 32) m |= 1u << d;
-        }
-        return m;
+        return a.v ? __ldg(xrow + a.i * nbw + bj) : ~0u;
     }
 
     template <bool HB>
@@ -358,7 +360,7 @@ struct Engine {
         const float Rc2 = CUT ? P.Rc2 : 3.0e38f, kq = P.kq_rc2;
         const float rc = CUT ? sqrtf(1.f / kq) : 0.f;
         const int i = bi * 32 + lane;
-        const TileAtom a = tile_atom(i, spos, sREQ, pbc, central);
+        const TileAtom a = tile_atom(i, spos, sREQ);
         const uint32_t xm = tile_mask(a, bj);
         float3 fi = make_float3(0.f, 0.f, 0.f), rj = make_float3(0.f, 0.f, 0.f);
         bool ok;
@@ -393,7 +395,7 @@ struct Engine {
         const float Rc2 = CUT ? P.Rc2 : 3.0e38f, kq = P.kq_rc2;
         const float rc = CUT ? sqrtf(1.f / kq) : 0.f;
         const int i = b * 32 + lane;
-        const TileAtom a = tile_atom(i, spos, sREQ, pbc, central);
+        const TileAtom a = tile_atom(i, spos, sREQ);
         const uint32_t xm = tile_mask(a, b);
         float3 fi = make_float3(0.f, 0.f, 0.f);
         bool ok;
@@ -662,7 +664,8 @@ struct Engine {
             BondedOut o;
             eval_atom<ENERGY>(ia, natoms, nnode, flags, P.Fmax2NB, spos, sREQ, ngs(ia), ngc(ia),
                               npar(L.apar, Y.apars, ia), npar(L.bL, Y.bLs, ia), npar(L.bK, Y.bKs, ia),
-                              npar(L.ksp, Y.Ksp, ia), npar(L.kpp, Y.Kpp, ia), lv, P.npbc[0], P.npbc[1], P.npbc[2], o);
+                              npar(L.ksp, Y.Ksp, ia), npar(L.kpp, Y.Kpp, ia), lv, P.npbc[0], P.npbc[1], P.npbc[2],
+                              __ldg(Y.a13 + noff + ia), Cut13(P), o);
             fasm[ia] = make_float4(o.fa.x, o.fa.y, o.fa.z, 0.f);
             fasm[natoms + ia] = make_float4(o.fpi.x, o.fpi.y, o.fpi.z, 0.f);
 #pragma unroll
@@ -670,7 +673,7 @@ struct Engine {
                 fng[ia * 4 + k] = make_float4(o.fbs[k].x, o.fbs[k].y, o.fbs[k].z, 0.f);
                 fng[4 * L.maxNN + ia * 4 + k] = make_float4(o.fps[k].x, o.fps[k].y, o.fps[k].z, 0.f);
             }
-            if (ENERGY) Eb += (double)o.E;
+            if (ENERGY) { Eb += (double)o.E; e13 += (double)o.E13; }
         }
         // --- non-bonded pairs: S lanes per atom i, j strided by S
         if (flags & F_NONBONDED) {
@@ -811,6 +814,7 @@ struct Engine {
             fmax2 = fmaxf(fmax2, (float)f2);
             bad |= !isfinite(f.x + f.y + f.z);
         }
+        bad |= pairbad;
     }
 
     // block reduction of 3 doubles + one float max (+flag); result in all threads
@@ -1028,12 +1032,17 @@ __global__ void __launch_bounds__(T) eval_kernel(Params P, Systems Y, const int*
     const float4* fasm = E.template at<float4>(L.fasm);
     for (int v = threadIdx.x; v < E.nvecs; v += T) Y.force[E.voff + v] = fasm[v];
     if (ENERGY) {
-        double eb = Eb, enb = Enb, eg = Eg;
+        // the reference's split: the skipped 1-3 pair energies belong to the
+        // pair sum and their subtraction to the bonded part; the total is
+        // summed without them
+        double eb = Eb, enb = Enb, eg = Eg, x13 = E.e13, z0 = 0.0, z1 = 0.0;
         float dummy = 0.f;
         bool b2 = false;
         __syncthreads();
         E.reduce4(eb, enb, eg, dummy, b2);
-        if (threadIdx.x == 0) Y.energy[s] = make_double4(eb, enb, eg, eb + enb + eg);
+        __syncthreads();
+        E.reduce4(x13, z0, z1, dummy, b2);
+        if (threadIdx.x == 0) Y.energy[s] = make_double4(eb - x13, enb + x13, eg, eb + enb + eg);
     }
     if (threadIdx.x == 0) Y.fconv[s] = sqrtf(fmax2);
 }

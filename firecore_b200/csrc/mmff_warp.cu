@@ -43,7 +43,8 @@ __device__ __forceinline__ float eval_atom_slots(int ia, int natoms, int nnode, 
                                                  const float4* sp, const float4* sREQ, int4 ng, int4 ngC,
                                                  const float4* gap, const float* gbL, const float* gbK,
                                                  const float* gKsp, const float* gKpp, const float* lv, int npx, int npy,
-                                                 int npz, float4* fbs, float4* fps, float3& fa_out, float3& fpi_out) {
+                                                 int npz, int a13, const Cut13& cu, float4* fbs, float4* fps,
+                                                 float3& fa_out, float3& fpi_out, float& E13) {
     const float3 pa = f3(sp[ia]);
     const float3 hpi = f3(sp[natoms + ia]);
     const float4 apar = *gap;
@@ -51,6 +52,7 @@ __device__ __forceinline__ float eval_atom_slots(int ia, int natoms, int nnode, 
     float3 hf[4];
     float he[4], hl[4];
     float E = 0.f;
+    E13 = 0.f;
     const int ings[4] = {ng.x, ng.y, ng.z, ng.w};
     const int ingC[4] = {ngC.x, ngC.y, ngC.z, ngC.w};
     auto addslot = [](float4* slot, float3 v) { float4 t = *slot; t.x += v.x; t.y += v.y; t.z += v.z; *slot = t; };
@@ -147,15 +149,17 @@ __device__ __forceinline__ float eval_atom_slots(int ia, int natoms, int nnode, 
                 float3 f2 = make_float3(h.x * fr2 + hf[j].x * (fr2 * c2), h.y * fr2 + hf[j].y * (fr2 * c2), h.z * fr2 + hf[j].z * (fr2 * c2));
                 fa = fa - (f1 + f2);
                 if (flags & F_SUB_ANGLE_NB) {
-                    const float4 Ri = sREQ[ings[i]], Rj = sREQ[ings[j]];
                     const float3 dp = hf[j] * hl[j] - hf[i] * hl[i];
-                    float e;
-                    const float F = ljqh<ENERGY>(dot3(dp, dp), Ri.x + Rj.x, Ri.y * Rj.y, Ri.z * Rj.z, fminf(Ri.w * Rj.w, 0.f), e);
+                    // x13: the pair sum skipped this central-image pair (pair13, mmff_device.cuh)
+                    const bool x13 = (flags & F_EXCL13) && ((a13 >> angle_slot(i, j)) & 1) &&
+                                     (!(flags & F_PBC) || ingC[i] == ingC[j]);
+                    float e = 0.f, ep = 0.f;
+                    const float F = pair13<ENERGY>(dot3(dp, dp), sREQ[ings[i]], sREQ[ings[j]], x13, cu.Rc2, cu.kq, cu.rc, e, ep);
                     float3 fij = dp * F;
                     if (flags & F_CLAMP_NB) { float ff = dot3(fij, fij); if (ff > Fmax2) fij = fij * sqrtf(Fmax2 / ff); }
-                    if (ENERGY) E -= e;
-                    f1 = f1 - fij;
-                    f2 = f2 + fij;
+                    if (ENERGY) { E += e; E13 += ep; }
+                    f1 = f1 + fij;
+                    f2 = f2 - fij;
                 }
                 addslot(fbs + i, f1);
                 addslot(fbs + j, f2);
@@ -365,6 +369,9 @@ struct WarpEngine {
     // owned state (k = 0, 1): atom a_k = lane + 32k, node n_k = a_k if < NN
     float3 va[APL], vp[APL];        // velocities of own atoms / own pi vectors
     float3 fasm_a[APL], fasm_p[APL];// assembled forces of the current step
+    const uint32_t* xrow;           // central-image exclusion rows of the system (ceil(N/32) words per atom)
+    int nbw;                        // words per row
+    double e13 = 0.0;               // ENERGY: pair energies of the skipped 1-3 pairs (energy split)
     unsigned long long npair = 0;
 
     __device__ WarpEngine(const Params& p, const Systems& y, char* region, const WarpLayout& L, int maxNN_)
@@ -385,6 +392,8 @@ struct WarpEngine {
         const int4 d = Y.desc[s];
         aoff = d.x; noff = d.y; voff = d.z; N = d.w;
         NN = Y.nnode[s]; NV = N + NN;
+        xrow = Y.xmask + Y.moff[s];
+        nbw = (N + 31) >> 5;
         if (lane < 9) lv[lane] = Y.lvec[9 * s + lane];
         if (lane >= 9 && lane < 12) lv[lane] = comp(Y.gorg[s], lane - 9);
         bool h = false;
@@ -421,6 +430,13 @@ struct WarpEngine {
         for (int k = 0; k < 3; k++) { mn[k] = wmin_f(a[k]); mx[k] = wmax_f(b[k]); }
     }
 
+    // central-image exclusion words of atom a (all set beyond the system)
+    __device__ __forceinline__ void central_rows(int a, uint32_t& lo, uint32_t& hi) const {
+        if (a >= N) { lo = hi = ~0u; return; }
+        lo = __ldg(xrow + a * nbw);
+        hi = nbw > 1 ? __ldg(xrow + a * nbw + 1) : ~0u;
+    }
+
     // forces of one step; assembled forces of owned vectors end in fasm_a/fasm_p
     __device__ void forces(double& Eb, double& Enb, double& Eg) {
         const int flags = P.flags;
@@ -432,12 +448,14 @@ struct WarpEngine {
             const int ia = lane + 32 * k;
             if (ia < NN) {
                 const float4* np_ = spar + 5 * ia;
+                float E13;
                 const float e = eval_atom_slots<ENERGY>(
                     ia, N, NN, flags, P.Fmax2NB, sp, sR, sng[ia], sngC[ia], np_, reinterpret_cast<const float*>(np_ + 1),
                     reinterpret_cast<const float*>(np_ + 2), reinterpret_cast<const float*>(np_ + 3),
                     reinterpret_cast<const float*>(np_ + 4), lv, P.npbc[0], P.npbc[1], P.npbc[2],
-                    fng + ia * 4, fng + 4 * maxNN + ia * 4, fa_own[k], fpi_own[k]);
-                if (ENERGY) Eb += (double)e;
+                    __ldg(Y.a13 + noff + ia), Cut13(P), fng + ia * 4, fng + 4 * maxNN + ia * 4, fa_own[k], fpi_own[k],
+                    E13);
+                if (ENERGY) { Eb += (double)e; e13 += (double)E13; }
             }
         }
         // ---- pairs, own atoms x all j
@@ -469,8 +487,13 @@ struct WarpEngine {
                         }
                         const int ipbc = ((iz + npz) * nyi + (iy + npy)) * nxi + (ix + npx);
                         uint32_t m0lo, m0hi, m1lo, m1hi;
-                        if (a0 < N) excl_mask(a0, sng[a0], sngC[a0], ipbc, pbc, m0lo, m0hi); else { m0lo = m0hi = ~0u; }
-                        if (APL == 2 && a1 < N) excl_mask(a1, sng[a1], sngC[a1], ipbc, pbc, m1lo, m1hi); else { m1lo = m1hi = ~0u; }
+                        if ((ix | iy | iz) == 0) {      // central image: the exclusion rows (bonded and 1-3 pairs)
+                            central_rows(a0, m0lo, m0hi);
+                            if (APL == 2) central_rows(a1, m1lo, m1hi); else { m1lo = m1hi = ~0u; }
+                        } else {
+                            if (a0 < N) excl_mask(a0, sng[a0], sngC[a0], ipbc, pbc, m0lo, m0hi); else { m0lo = m0hi = ~0u; }
+                            if (APL == 2 && a1 < N) excl_mask(a1, sng[a1], sngC[a1], ipbc, pbc, m1lo, m1hi); else { m1lo = m1hi = ~0u; }
+                        }
                         if (APL == 2 && (ix | iy | iz) == 0) {      // central image: each pair once
                             if (hasH) central_pairs<ENERGY, COUNT, true>(P, N, lane, sp, sR, m0lo, m0hi, m1lo, m1hi, f0, f1, ec, npair);
                             else central_pairs<ENERGY, COUNT, false>(P, N, lane, sp, sR, m0lo, m0hi, m1lo, m1hi, f0, f1, ec, npair);
@@ -747,8 +770,12 @@ __global__ void __launch_bounds__(128) eval_warp_kernel(Params P, Systems Y, con
     }
     fm = wmax_f(fm);
     if (ENERGY) {
+        // the reference's split: the skipped 1-3 pair energies belong to the
+        // pair sum and their subtraction to the bonded part; the total is
+        // summed without them
+        const double e13 = wsum_d(E.e13);
         Eb = wsum_d(Eb); Enb = wsum_d(Enb); Eg = wsum_d(Eg);
-        if (lane == 0) Y.energy[s] = make_double4(Eb, Enb, Eg, Eb + Enb + Eg);
+        if (lane == 0) Y.energy[s] = make_double4(Eb - e13, Enb + e13, Eg, Eb + Enb + Eg);
     }
     if (lane == 0) Y.fconv[s] = sqrtf(fm);
 }

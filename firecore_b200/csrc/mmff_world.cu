@@ -8,6 +8,7 @@
 // buckets and launches one persistent relaxation kernel per bucket.
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -42,6 +43,10 @@ using namespace mmff;
 namespace {
 
 std::string g_err;
+// kernels this library launched (relaxation, evaluation, learned proposal);
+// a graph replay counts every kernel node it runs
+std::atomic<unsigned long long> g_launches{0};
+bool g_capturing = false;      // enqueue_relax inside a graph capture: counted at replay
 int fail(const char* fmt, ...) {
     char buf[512];
     va_list ap; va_start(ap, fmt); vsnprintf(buf, sizeof buf, fmt, ap); va_end(ap);
@@ -100,6 +105,11 @@ struct World {
     DBuf<int4> d_desc; DBuf<int> d_nnode; DBuf<float> d_lvec; DBuf<float4> d_gorg;
     DBuf<float4> d_REQ, d_PLQ; DBuf<int4> d_ng, d_ngC, d_bk;
     DBuf<float4> d_apar, d_bL, d_bK, d_ksp, d_kpp;
+    // 1-3 pairs and central-image exclusion rows (built for the current flags and image set)
+    std::vector<int4> h_ng, h_ngC;
+    std::vector<int> h_a13;
+    DBuf<int> d_a13, d_moff;
+    DBuf<uint32_t> d_xmask;
     DBuf<float4> d_pos, d_vel, d_force, d_pos0, d_vel0;
     DBuf<double4> d_fire, d_fire0, d_energy;
     DBuf<int> d_status, d_nsteps, d_counter;
@@ -153,7 +163,8 @@ int ensure_ready() {
 Params make_params(bool for_eval, int nstep_max, double Fconv, int conv_mode) {
     Params P;
     memset(&P, 0, sizeof P);
-    P.flags = W.flags;
+    P.flags = W.flags & ~F_EXCL13;
+    if (excl13_active(P.flags)) P.flags |= F_EXCL13;
     if (!W.grid.p) P.flags &= ~F_GRID;
     for (int k = 0; k < 3; k++) P.npbc[k] = W.npbc[k];
     P.Rc2 = W.Rcut > 0 ? (float)(W.Rcut * W.Rcut) : 0.f;
@@ -190,6 +201,7 @@ Systems make_systems() {
     Y.desc = W.d_desc.p; Y.nnode = W.d_nnode.p; Y.lvec = W.d_lvec.p; Y.gorg = W.d_gorg.p;
     Y.REQ = W.d_REQ.p; Y.PLQ = W.d_PLQ.p; Y.neighs = W.d_ng.p; Y.neighCell = W.d_ngC.p; Y.bkneighs = W.d_bk.p;
     Y.apars = W.d_apar.p; Y.bLs = W.d_bL.p; Y.bKs = W.d_bK.p; Y.Ksp = W.d_ksp.p; Y.Kpp = W.d_kpp.p;
+    Y.a13 = W.d_a13.p; Y.xmask = W.d_xmask.p; Y.moff = W.d_moff.p;
     Y.pos = W.d_pos.p; Y.vel = W.d_vel.p; Y.force = W.d_force.p; Y.fire = W.d_fire.p;
     Y.status = W.d_status.p; Y.nsteps = W.d_nsteps.p; Y.fconv = W.d_fconv.p; Y.energy = W.d_energy.p;
     Y.counters = W.d_stats.p;
@@ -275,6 +287,89 @@ void default_config(int cls, int maxNA, int& kind, int& apl, int& T, int& S) {
     if (W.force_S) S = W.force_S;
 }
 
+template <class X> int upload(DBuf<X>& d, const std::vector<X>& h) {
+    if (d.ensure(h.size())) return -1;
+    if (!h.empty()) CK(cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(X), cudaMemcpyHostToDevice, W.stream));
+    return 0;
+}
+
+// Angle pairs whose 1-3 pair the pair sum may skip (per node, bit
+// angle_slot(i, j) of neighbour slots i < j): the two ends are different
+// atoms, not bonded to each other, and no other angle of the system has the
+// same two ends (rings of three or four atoms keep the reference's add-then-
+// subtract form).  Topology only; whether the pair is central is decided per
+// step from the neighbour cells.
+void angle_pairs13(int na, int nn, const int4* ng, int* a13) {
+    std::vector<long long> ends, bonds;
+    auto key = [](int a, int b) { return a < b ? (long long)a << 32 | (unsigned)b : (long long)b << 32 | (unsigned)a; };
+    for (int i = 0; i < na; i++) {
+        const int g[4] = {ng[i].x, ng[i].y, ng[i].z, ng[i].w};
+        for (int k = 0; k < 4; k++) if (g[k] >= 0) bonds.push_back(key(i, g[k]));
+    }
+    for (int ia = 0; ia < nn; ia++) {
+        const int g[4] = {ng[ia].x, ng[ia].y, ng[ia].z, ng[ia].w};
+        for (int i = 0; i < 3; i++) for (int j = i + 1; j < 4; j++)
+            if (g[i] >= 0 && g[j] >= 0) ends.push_back(key(g[i], g[j]));
+    }
+    std::sort(ends.begin(), ends.end());
+    std::sort(bonds.begin(), bonds.end());
+    for (int ia = 0; ia < nn; ia++) {
+        const int g[4] = {ng[ia].x, ng[ia].y, ng[ia].z, ng[ia].w};
+        int m = 0;
+        for (int i = 0; i < 3; i++) for (int j = i + 1; j < 4; j++) {
+            if (g[i] < 0 || g[j] < 0 || g[i] == g[j]) continue;
+            const long long k = key(g[i], g[j]);
+            const auto r = std::equal_range(ends.begin(), ends.end(), k);
+            if (r.second - r.first != 1 || std::binary_search(bonds.begin(), bonds.end(), k)) continue;
+            m |= 1 << angle_slot(i, j);
+        }
+        a13[ia] = m;
+    }
+}
+
+// Central-image exclusion rows of every system for the current flags and
+// image set: per atom i, ceil(natoms/32) words whose bit j marks a pair the
+// central-image pair sum skips -- i itself, padding slots j >= natoms, bonded
+// neighbours in the central cell (NBFF.h:590-607; both directions), and with
+// F_EXCL13 the central 1-3 pairs of angle_pairs13 (their angle terms carry
+// them, pair13).  Rows are symmetric.
+int build_xmask() {
+    const bool pbc = (W.flags & F_PBC) != 0;
+    const bool x13 = excl13_active(W.flags);
+    const int nxi = 2 * W.npbc[0] + 1, nyi = 2 * W.npbc[1] + 1;
+    const int central = (W.npbc[2] * nyi + W.npbc[1]) * nxi + W.npbc[0];
+    std::vector<int> moff(W.nsys);
+    size_t tot = 0;
+    for (int s = 0; s < W.nsys; s++) { moff[s] = (int)tot; tot += (size_t)W.natoms[s] * ((W.natoms[s] + 31) / 32); }
+    if (tot > (size_t)INT32_MAX) return fail("exclusion rows too large (%zu words)", tot);
+    std::vector<uint32_t> m(tot, 0u);
+    for (int s = 0; s < W.nsys; s++) {
+        const int na = W.natoms[s], nn = W.nnode[s], a0 = W.desc[s].x, n0 = W.desc[s].y, nb = (na + 31) / 32;
+        uint32_t* row = m.data() + moff[s];
+        auto set = [&](int i, int j) { row[i * nb + (j >> 5)] |= 1u << (j & 31); };
+        for (int i = 0; i < na; i++) {
+            set(i, i);
+            for (int j = na; j < 32 * nb; j++) set(i, j);
+            const int4 g = W.h_ng[a0 + i], c = W.h_ngC[a0 + i];
+            const int gg[4] = {g.x, g.y, g.z, g.w}, cc[4] = {c.x, c.y, c.z, c.w};
+            for (int k = 0; k < 4; k++)
+                if (gg[k] >= 0 && (!pbc || cc[k] == central)) { set(i, gg[k]); set(gg[k], i); }
+        }
+        if (!x13) continue;
+        for (int ia = 0; ia < nn; ia++) {
+            const int bits = W.h_a13[n0 + ia];
+            if (!bits) continue;
+            const int4 g = W.h_ng[a0 + ia], c = W.h_ngC[a0 + ia];
+            const int gg[4] = {g.x, g.y, g.z, g.w}, cc[4] = {c.x, c.y, c.z, c.w};
+            for (int i = 0; i < 3; i++) for (int j = i + 1; j < 4; j++)
+                if (((bits >> angle_slot(i, j)) & 1) && (!pbc || cc[i] == cc[j])) { set(gg[i], gg[j]); set(gg[j], gg[i]); }
+        }
+    }
+    if (upload(W.d_moff, moff) || upload(W.d_xmask, m)) return -1;
+    CK(cudaStreamSynchronize(W.stream));
+    return 0;
+}
+
 int build_buckets() {
     for (auto& B : W.buckets) B.queue.release();
     W.buckets.clear();
@@ -301,6 +396,7 @@ int build_buckets() {
         cudaStream_t s; CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); W.bstreams.push_back(s);
         cudaEvent_t e; CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming)); W.bev.push_back(e);
     }
+    if (build_xmask()) return -1;
     W.buckets_dirty = false;
     return 0;
 }
@@ -321,11 +417,6 @@ struct PinnedBuf {
 };
 PinnedBuf g_stage_a, g_stage_b;
 
-template <class X> int upload(DBuf<X>& d, const std::vector<X>& h) {
-    if (d.ensure(h.size())) return -1;
-    if (!h.empty()) CK(cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(X), cudaMemcpyHostToDevice, W.stream));
-    return 0;
-}
 
 // the launches of one relax call on the library stream: reset the work
 // counters, fork to one stream per bucket, one persistent kernel per bucket
@@ -346,6 +437,7 @@ int enqueue_relax(const Params& P) {
         int mna = B.maxNA, mnn = B.maxNN;
         void* args[] = {&Pc, &Y, &q, &nq, &ctr, &mna, &mnn};
         CK(cudaLaunchKernel(fn, dim3(B.grid), dim3(B.T), args, B.smem, st));
+        if (!g_capturing) g_launches++;
     }
     for (size_t b = 0; b < W.buckets.size(); b++) {
         CK(cudaEventRecord(W.bev[b], W.bstreams[b]));
@@ -358,6 +450,7 @@ int enqueue_relax(const Params& P) {
 }  // namespace
 
 void mmff_set_error(const char* msg) { g_err = msg; }
+void mmff_count_launches(int n) { g_launches += (unsigned long long)n; }
 
 namespace mmff {
 
@@ -366,6 +459,7 @@ cudaStream_t world_stream() { return ensure_ready() ? nullptr : W.stream; }
 int world_view(WorldView* v) {
     if (ensure_ready()) return -1;
     if (!W.nsys) return fail("no systems uploaded");
+    if (W.buckets_dirty && build_buckets()) return -1;     // exclusion rows of the current systems
     v->P = make_params(true, 0, 0.0, 0);
     v->Y = make_systems();
     v->stream = W.stream;
@@ -381,6 +475,8 @@ int world_view(WorldView* v) {
 extern "C" {
 
 const char* mmff_last_error(void) { return g_err.c_str(); }
+
+unsigned long long mmff_kernel_launches(void) { return g_launches.load(); }
 
 int mmff_init_device(int device) {
     if (W.ready && W.device == device) return 0;
@@ -520,6 +616,7 @@ int mmff_systems_upload(int nsys, const int* natoms, const int* nnode, const dou
     W.orig.assign(3 * nsys, 0.0);
     std::vector<float4> hpos(NV), hvel(NV), hREQ(NA), hPLQ(NA), hap(NN), hbL(NN), hbK(NN), hks(NN), hkp(NN), hgorg(nsys);
     std::vector<int4> hng(NA), hngC(NA), hbk(NA);
+    std::vector<int> ha13(NN);
     std::vector<float> hlv(9 * nsys);
     std::vector<double4> hfire(nsys);
     const double sqk = std::sqrt(14.3996448915);
@@ -550,6 +647,7 @@ int mmff_systems_upload(int nsys, const int* natoms, const int* nnode, const dou
             auto f4 = [&](const double* a) { return make_float4((float)a[4 * (n0 + i)], (float)a[4 * (n0 + i) + 1], (float)a[4 * (n0 + i) + 2], (float)a[4 * (n0 + i) + 3]); };
             hap[n0 + i] = f4(apars); hbL[n0 + i] = f4(bLs); hbK[n0 + i] = f4(bKs); hks[n0 + i] = f4(Ksp); hkp[n0 + i] = f4(Kpp);
         }
+        angle_pairs13(na, nn, &hng[a0], &ha13[n0]);
         for (int k = 0; k < 9; k++) hlv[9 * s + k] = (float)lvec[9 * s + k];
         hgorg[s] = make_float4((float)(c[0] - W.gpos0[0]), (float)(c[1] - W.gpos0[1]), (float)(c[2] - W.gpos0[2]), 0.f);
         hfire[s] = make_double4(W.fire[0], W.fire[2], 0.0, 0.0);
@@ -559,8 +657,10 @@ int mmff_systems_upload(int nsys, const int* natoms, const int* nnode, const dou
         upload(W.d_REQ, hREQ) || upload(W.d_PLQ, hPLQ) || upload(W.d_ng, hng) || upload(W.d_ngC, hngC) ||
         upload(W.d_bk, hbk) || upload(W.d_apar, hap) || upload(W.d_bL, hbL) || upload(W.d_bK, hbK) ||
         upload(W.d_ksp, hks) || upload(W.d_kpp, hkp) || upload(W.d_pos, hpos) || upload(W.d_vel, hvel) ||
-        upload(W.d_pos0, hpos) || upload(W.d_vel0, hvel) || upload(W.d_fire, hfire) || upload(W.d_fire0, hfire))
+        upload(W.d_pos0, hpos) || upload(W.d_vel0, hvel) || upload(W.d_fire, hfire) || upload(W.d_fire0, hfire) ||
+        upload(W.d_a13, ha13))
         return -1;
+    W.h_ng = std::move(hng); W.h_ngC = std::move(hngC); W.h_a13 = std::move(ha13);
     if (W.d_force.ensure(NV) || W.d_energy.ensure(nsys) || W.d_status.ensure(nsys) || W.d_nsteps.ensure(nsys) ||
         W.d_fconv.ensure(nsys) || W.d_counter.ensure(64) || W.d_stats.ensure(8))
         return -1;
@@ -624,6 +724,7 @@ int mmff_eval(int with_energy) {
         void* args[] = {&P, &Y, &q, &nq, &mna, &mnn};
         const int nblk = B.kind ? (nq + 3) / 4 : nq;
         CK(cudaLaunchKernel(fn, dim3(nblk), dim3(B.T), args, B.smem, W.stream));
+        g_launches++;
     }
     CK(cudaGetLastError());
     return 0;
@@ -645,7 +746,9 @@ int mmff_relax(int nstep_max, double Fconv, int conv_mode) {
         if (W.gexec) { cudaGraphExecDestroy(W.gexec); W.gexec = nullptr; }
         cudaGraph_t g = nullptr;
         CK(cudaStreamBeginCapture(W.stream, cudaStreamCaptureModeThreadLocal));
+        g_capturing = true;
         const int rc = enqueue_relax(P);
+        g_capturing = false;
         const cudaError_t e = cudaStreamEndCapture(W.stream, &g);
         if (rc) { if (g) cudaGraphDestroy(g); cudaGetLastError(); return -1; }
         if (e != cudaSuccess) return fail("relax graph capture: %s", cudaGetErrorString(e));
@@ -656,6 +759,7 @@ int mmff_relax(int nstep_max, double Fconv, int conv_mode) {
         W.gkey_count = W.count; W.gkey_version = W.version;
     }
     CK(cudaGraphLaunch(W.gexec, W.stream));
+    g_launches += W.buckets.size();
     return 0;
 }
 
@@ -742,6 +846,8 @@ int mmff_autotune(int nstep_probe, int max_sample, float* report, int report_cap
     if (!W.nsys) return fail("no systems uploaded");
     if (nstep_probe < 1 || max_sample < 1) return fail("autotune: nstep_probe and max_sample must be >= 1");
     if (W.force_T || W.force_S) return fail("autotune: clear mmff_set_launch overrides first");
+    // the candidate kernels read the exclusion rows of the current systems
+    if (W.buckets_dirty && build_buckets()) return -1;
     DBuf<float4> sp, sv; DBuf<double4> sf; DBuf<int> sst, sns; DBuf<float> sfc;
     if (sp.ensure(W.NV) || sv.ensure(W.NV) || sf.ensure(W.nsys) || sst.ensure(W.nsys) || sns.ensure(W.nsys) ||
         sfc.ensure(W.nsys))
@@ -787,6 +893,7 @@ int mmff_autotune(int nstep_probe, int max_sample, float* report, int report_cap
                     CK(cudaMemsetAsync(ctr, 0, sizeof(int), W.stream));
                     CK(cudaEventRecord(W.ev0, W.stream));
                     CK(cudaLaunchKernel(fn, dim3(B.grid), dim3(B.T), args, B.smem, W.stream));
+                    g_launches++;
                     CK(cudaEventRecord(W.ev1, W.stream));
                     CK(cudaEventSynchronize(W.ev1));
                     CK(cudaEventElapsedTime(&ms, W.ev0, W.ev1));

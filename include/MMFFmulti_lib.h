@@ -27,6 +27,11 @@ extern "C" {
 
 /* ------------------------------------------------------------ errors/setup */
 const char* mmff_last_error(void);
+/* No counterpart in the reference.  Kernels this library has launched so far
+ * on the relaxation, evaluation and learned-proposal paths (a replay of the
+ * captured relax graph counts each kernel it runs); callers difference two
+ * readings to count the launches of a region. */
+unsigned long long mmff_kernel_launches(void);
 /* Select the CUDA device and create the library stream.
  * Replaces OCLsystem::init (cpp/common/OpenCL/OCL.h:386-410). */
 int mmff_init_device(int device);
@@ -79,11 +84,14 @@ int mmff_grid_build(int nsub, const double* spos, const double* sREQ, const doub
  * Limit: at most 4096 points per axis (larger grids return an error).  The
  * solver coefficients live in one static device array per GPU that the
  * library keeps until exit; every call rewrites them before use, and calls
- * whose kernels overlap on the GPU (different streams) race on it.  The
- * first call on a device looks up that array's device address
- * (cudaGetSymbolAddress) with the device current; make that first call
- * before any stream capture.  Kernels run on `stream` (a cudaStream_t;
- * NULL = legacy default stream); the call does not synchronise. */
+ * whose kernels overlap on the GPU (different streams) race on it.  Every
+ * call looks up that array's device address (cudaGetSymbolAddress) on the
+ * current device, so a reset or recreated context is picked up; the first
+ * call on a device also loads the library's kernels there, so make it before
+ * any stream capture.  d_coefs must be device (or managed) memory of the
+ * current device; anything else returns an error before any launch.
+ * Kernels run on `stream` (a cudaStream_t; NULL = legacy default stream);
+ * the call does not synchronise. */
 int mmff_bspline_fit_noalloc(double* d_coefs, int nx, int ny, int nz, void* stream);
 /* B-spline sample (GridFF::getForce_Bspline, GridFF.h:355) at n points:
  * pos [n*3], PLQ [n*4] -> fe [n*4] = (Fx, Fy, Fz, E). */

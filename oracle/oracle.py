@@ -53,8 +53,9 @@ def build_oracle(with_ref: bool = False):
     """Compile the checkers (make in oracle/); the reference harness only where
     the reference tree is present."""
     subprocess.check_call(["make", "-s", "-C", HERE, "all"])
-    if with_ref and os.path.isdir("/root/reference/cpp"):
-        subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
+    ref_root = os.environ.get("REF_ROOT", "/root/reference")
+    if with_ref and os.path.isdir(os.path.join(ref_root, "cpp")):
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref", f"REF_ROOT={ref_root}"])
 
 
 def orc():
