@@ -73,6 +73,7 @@ def _declare(lib):
         "mmff_grid_sample": [c_int, c_void, c_void, c_void],
         "mmff_systems_upload": [c_int] + [c_void] * 14, "mmff_systems_restore": [],
         "mmff_systems_set_state": [c_void, c_void, c_int], "mmff_eval": [c_int],
+        "mmff_set_constraints": [c_void, c_void], "mmff_set_grid_cache": [c_int],
         "mmff_relax": [c_int, c_double, c_int], "mmff_get_forces": [c_void], "mmff_get_energies": [c_void],
         "mmff_get_state": [c_void] * 6, "mmff_timer_start": [], "mmff_num_buckets": [],
         "mmff_bucket_info": [c_int, c_void], "mmff_set_counting": [c_int], "mmff_get_counters": [c_void],
@@ -81,6 +82,7 @@ def _declare(lib):
         "mmff_mlp_infer": [c_int, c_void, c_void], "mmff_mlp_set_data": [c_int, c_void, c_void],
         "mmff_mlp_train": [c_int, c_int, c_double, c_double, c_void], "mmff_mlp_set_elements": [c_void],
         "mmff_mlp_features": [c_double, c_void], "mmff_mlp_warmstart": [c_int, c_double, c_void],
+        "mmff_mlp_set_projection": [c_int], "mmff_mlp_project": [c_void, c_void],
         "mmff_mlp_plan": [c_void], "mmff_mlp_layout": [c_void],
         "mmff_set_graph": [c_int], "mmff_set_md": [c_double, c_double, c_double, ctypes.c_ulonglong],
         "mmff_md": [c_int], "mmff_surf_upload": [c_int, c_void, c_void, c_void, c_void, c_double], "mmff_autotune": [c_int, c_int, c_void, c_int],

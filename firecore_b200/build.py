@@ -3,6 +3,11 @@
 Compiles every ``csrc/*.cu`` and ``csrc/*.cpp`` with nvcc for sm_100a and links
 one shared library in-tree, so the built file travels with the source tree.
 The C-ABI it exports is declared in ``include/MMFFmulti_lib.h``.
+
+The seeded workload generator (``csrc/molgen.cpp``) is also linked on its own
+into the host-only ``libmmff_gen.so`` (no CUDA): inputs for CPU-only consumers
+(the reference timing arm) come from the same code without mapping the GPU
+library.
 """
 import glob
 import os
@@ -15,6 +20,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(ROOT, "_build")
 LIB = os.path.join(HERE, "libMMFFmulti_lib.so")
+GEN_LIB = os.path.join(HERE, "libmmff_gen.so")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 HOST_CXX = "/usr/bin/g++"
@@ -58,6 +64,12 @@ def build(verbose=False, force=False):
         # so the library also loads (without computing) on hosts without a GPU.
         cmd = [NVCC] + ARCH + ["-shared", "-ccbin", HOST_CXX, "-Xcompiler", "-fopenmp", "-o", LIB] + objs + \
             ["-lcudart_static", "-lgomp"]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.check_call(cmd)
+    gen_src = os.path.join(CSRC, "molgen.cpp")
+    if force or _needs(GEN_LIB, [gen_src] + headers):
+        cmd = [HOST_CXX] + CXX_FLAGS + ["-shared", "-o", GEN_LIB, gen_src, "-lgomp"]
         if verbose:
             print(" ".join(cmd))
         subprocess.check_call(cmd)

@@ -30,6 +30,8 @@ enum : int {
     // are left out of the central-image pair sum instead of being added there
     // and subtracted again in the angle term (see pair13)
     F_EXCL13 = 1 << 11,
+    // set by the host for relaxations when position constraints are uploaded
+    F_CONSTR = 1 << 12,
 };
 
 // The host turns F_EXCL13 on exactly when the angle terms subtract the 1-3
@@ -109,6 +111,10 @@ struct Systems {
     const int* __restrict__ a13;        // per node: angle pairs (bit t of slots i<j) whose 1-3 pair the pair sum skips
     const uint32_t* __restrict__ xmask; // central-image exclusion words: row (atom i) of ceil(natoms/32) words per system
     const int* __restrict__ moff;       // per system: first word of its exclusion rows
+    const float4* __restrict__ constr;  // per atom: spring anchor (local frame) and w > 0 = on (F_CONSTR)
+    const float4* __restrict__ constrK; // per atom: spring constants (kx, ky, kz)
+    unsigned int* gkey;                 // per atom: stencil cell of its GridFF cache (0xffffffff: empty); null: no cache
+    float4* gcs;                        // per atom: 16 float4 = PLQ . C of its 4x4x4 stencil ([x][y] rows of 4 z)
     float4* pos;                        // local frame
     float4* vel;
     float4* force;                      // assembled forces (written by eval / at exit)
@@ -274,6 +280,20 @@ struct Cut13 {
     }
 };
 
+// Position constraint of one atom (relax_multi.cl:995-1010, updateAtomsMMFFf4):
+// with anchor.w > 0 the force gains (anchor - p) * max(K, 0) per component,
+// after the force clamp; pi orbitals have none.
+__device__ __forceinline__ float3 constraint_force(const Systems& Y, int ia, float3 p, float3 f) {
+    const float4 c = __ldg(Y.constr + ia);
+    if (c.w > 0.f) {
+        const float4 k = __ldg(Y.constrK + ia);
+        f.x = fmaf(c.x - p.x, fmaxf(k.x, 0.f), f.x);
+        f.y = fmaf(c.y - p.y, fmaxf(k.y, 0.f), f.y);
+        f.z = fmaf(c.z - p.z, fmaxf(k.z, 0.f), f.z);
+    }
+    return f;
+}
+
 // angle pair index of neighbour slots i < j (0..5): (0,1) (0,2) (0,3) (1,2) (1,3) (2,3)
 __host__ __device__ constexpr int angle_slot(int i, int j) { return i * (7 - i) / 2 + (j - i - 1); }
 
@@ -431,6 +451,15 @@ __device__ __forceinline__ float4 bs_dbasis(float u) {
 }
 __device__ __forceinline__ float comp(float4 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w)); }
 
+// Grid coordinates of an atom far outside any grid (|u| >= 2^20 voxels: only
+// in a system that has blown up, which the relax kernels retire) or not
+// finite are replaced by the origin, so that the int conversions and the
+// periodic wraps below stay in range for every input.
+__device__ __forceinline__ float3 grid_safe(float3 u) {
+    const float lim = 1048576.f;
+    return (fabsf(u.x) < lim && fabsf(u.y) < lim && fabsf(u.z) < lim) ? u : make_float3(0.f, 0.f, 0.f);
+}
+
 // One x-slice (a = 0..3) of the 4x4x4 stencil of Bspline::fe3d_pbc_comb3 for
 // grid coordinate u (already in voxel units).  Returns the slice's partial
 // (dE/dx*bx', E-channel combos) as (Fx, Fy, Fz, E) *before* the -1/step scale.
@@ -441,6 +470,7 @@ __device__ __forceinline__ float comp(float4 v, int k) { return k == 0 ? v.x : (
 template <int UNROLL = 4>
 __device__ __forceinline__ float4 grid_slice(const float4* __restrict__ G, int nx, int ny, int nz, float3 u,
                                              float4 PLQ, int a) {
+    u = grid_safe(u);
     int ix = (int)u.x, iy = (int)u.y, iz = (int)u.z;
     if (u.x < 0.f) ix--;
     if (u.y < 0.f) iy--;
@@ -474,12 +504,73 @@ __device__ __forceinline__ float4 grid_slice(const float4* __restrict__ G, int n
     return make_float4(dxa * ez, bxa * ex, bxa * ey, bxa * ez);
 }
 
+// grid_slice with a per-atom cache of the 64 channel-combined coefficients
+// PLQ . C of the atom's stencil (PLQ is constant per atom).  An atom whose
+// stencil cell is the cached one reads its 16 numbers of slice a (4 float4,
+// 64 contiguous bytes) instead of gathering 16 float4 of the grid (256 B from
+// four columns); on a cell change the slice is gathered, combined and stored
+// as before.  The arithmetic is the same as grid_slice's, so results are
+// bit-identical.  All 32 lanes of the warp call it (a shuffle inside); the
+// four lanes of an atom are consecutive (lane a = lane & 3); ok = the lane
+// holds a real atom.  The cache of an atom is read and written only by the
+// block that owns its system in this launch; a block barrier separates steps.
+template <int UNROLL = 4>
+__device__ __forceinline__ float4 grid_slice_cached(const float4* __restrict__ G, int nx, int ny, int nz, float3 u,
+                                                    float4 PLQ, int a, bool ok, unsigned int* gkey, float4* gcs,
+                                                    int atom) {
+    u = grid_safe(u);
+    int ix = (int)u.x, iy = (int)u.y, iz = (int)u.z;
+    if (u.x < 0.f) ix--;
+    if (u.y < 0.f) iy--;
+    const float tx = u.x - (float)ix, ty = u.y - (float)iy, tz = u.z - (float)iz;
+    iz = min(max(iz, 3), nz - 5);
+    ix = wrap_index(ix - 1, nx);
+    iy = wrap_index(iy - 1, ny);
+    const unsigned key = ((unsigned)ix * 4096u + (unsigned)iy) * 256u + (unsigned)iz;
+    unsigned old = 0xffffffffu;
+    if (ok && a == 0) old = gkey[atom];
+    old = __shfl_sync(0xffffffffu, old, (threadIdx.x & 31) & ~3);
+    const bool hit = ok && old == key;
+    float4* mine = gcs + (size_t)atom * 16 + 4 * a;
+    int xa = ix + a; if (xa >= nx) xa -= nx;
+    const float4 bz = bs_basis(tz), dz = bs_dbasis(tz);
+    const float4 by = bs_basis(ty), dy = bs_dbasis(ty);
+    float ex = 0.f, ey = 0.f, ez = 0.f;
+#pragma unroll UNROLL
+    for (int b = 0; b < 4; b++) {
+        float4 cs;
+        if (hit) {
+            cs = mine[b];
+        } else {
+            int yb = iy + b; if (yb >= ny) yb -= ny;
+            const float4* col = G + ((size_t)(xa * ny + yb) * nz + (iz - 1));
+            const float4 c0 = __ldg(col), c1 = __ldg(col + 1), c2 = __ldg(col + 2), c3 = __ldg(col + 3);
+            cs.x = fmaf(PLQ.x, c0.x, fmaf(PLQ.y, c0.y, PLQ.z * c0.z));
+            cs.y = fmaf(PLQ.x, c1.x, fmaf(PLQ.y, c1.y, PLQ.z * c1.z));
+            cs.z = fmaf(PLQ.x, c2.x, fmaf(PLQ.y, c2.y, PLQ.z * c2.z));
+            cs.w = fmaf(PLQ.x, c3.x, fmaf(PLQ.y, c3.y, PLQ.z * c3.z));
+            if (ok) mine[b] = cs;
+        }
+        const float v = fmaf(bz.x, cs.x, fmaf(bz.y, cs.y, fmaf(bz.z, cs.z, bz.w * cs.w)));
+        const float d = fmaf(dz.x, cs.x, fmaf(dz.y, cs.y, fmaf(dz.z, cs.z, dz.w * cs.w)));
+        const float byb = comp(by, b), dyb = comp(dy, b);
+        ex = fmaf(v, dyb, ex);
+        ey = fmaf(d, byb, ey);
+        ez = fmaf(v, byb, ez);
+    }
+    if (ok && !hit && a == 0) gkey[atom] = key;
+    const float4 bx = bs_basis(tx), dx = bs_dbasis(tx);
+    const float bxa = comp(bx, a), dxa = comp(dx, a);
+    return make_float4(dxa * ez, bxa * ex, bxa * ey, bxa * ez);
+}
+
 // B-spline GridFF force + energy of one atom, the whole 4x4x4 stencil in this
 // lane (Bspline::fe3d_pbc_comb3, Bspline.h:742-809; the same index and basis
 // arithmetic as grid_slice)
 __device__ __forceinline__ float4 grid_atom(const Params& P, float3 u, float4 PLQ) {
     const int nx = P.gn[0], ny = P.gn[1], nz = P.gn[2];
     const float4* __restrict__ G = P.grid;
+    u = grid_safe(u);
     int ix = (int)u.x, iy = (int)u.y, iz = (int)u.z;
     if (u.x < 0.f) ix--;
     if (u.y < 0.f) iy--;

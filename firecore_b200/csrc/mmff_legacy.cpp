@@ -193,6 +193,9 @@ struct LegacyWorld {
     bool md_set = false;          // Langevin parameters passed to the device world
     // host mirrors (pyBall/MMFF_multi.py:238-256 shapes)
     std::vector<float> atoms, aforces, avel, constr, REQs, MMpars, BLs, BKs, Ksp, Kpp, lvecs, ilvecs, pbcshifts;
+    // spring constants of the constr anchors (MolWorld_sp3_multi::constrK): -1 = no
+    // force, as the reference initialises them (MolWorld_sp3_multi.h:224-225)
+    std::vector<float> constrK;
     std::vector<int> gneighs, gneighCell, gbkNeighs;
     // single-replica CPU-side buffers (getBuff names), replica iSystemCur
     std::vector<double> DOFs, fDOFs, vDOFs, Es;
@@ -244,8 +247,15 @@ int upload_all(bool params) {
     (void)params;
     if (mmff_set_params(L.bGrid ? L.flags : (L.flags & ~256), L.nPBC, -1.0, L.alphaMorse, 10.0)) return -1;
     if (mmff_set_fire(L.fire[0], L.fire[1], L.fire[2], L.fire[3], L.fire[4], L.fire[5], (int)L.fire[6], L.fire[7], L.fire[8], 0)) return -1;
-    return mmff_systems_upload(ns, natoms.data(), nnode.data(), pos.data(), vel.data(), ng.data(), ngC.data(), bk.data(),
-                               REQ.data(), ap.data(), bL.data(), bK.data(), ks.data(), kp.data(), lv.data());
+    if (mmff_systems_upload(ns, natoms.data(), nnode.data(), pos.data(), vel.data(), ng.data(), ngC.data(), bk.data(),
+                            REQ.data(), ap.data(), bL.data(), bK.data(), ks.data(), kp.data(), lv.data()))
+        return -1;
+    // the gpu_constr mirror (anchors, w > 0 = on) with its spring constants
+    std::vector<double> ca(4 * (size_t)ns * na), ck(4 * (size_t)ns * na);
+    bool any = false;
+    for (size_t i = 0; i < ca.size(); i++) { ca[i] = L.constr[i]; ck[i] = L.constrK[i]; }
+    for (size_t i = 0; i < (size_t)ns * na; i++) any |= ca[4 * i + 3] > 0 && (ck[4 * i] > 0 || ck[4 * i + 1] > 0 || ck[4 * i + 2] > 0);
+    return mmff_set_constraints(any ? ca.data() : nullptr, any ? ck.data() : nullptr);
 }
 
 // device state -> mirrors
@@ -403,6 +413,7 @@ void* init(int nSys, char* xyz_name, char* surf_name, char* smile_name, bool bMM
     // mirrors
     L.atoms.assign(4 * (size_t)nSys * nv, 0.f); L.aforces.assign(4 * (size_t)nSys * nv, 0.f); L.avel.assign(4 * (size_t)nSys * nv, 0.f);
     L.constr.assign(4 * (size_t)nSys * na, -1.f); L.REQs.assign(4 * (size_t)nSys * na, 0.f);
+    L.constrK.assign(4 * (size_t)nSys * na, -1.f);
     L.MMpars.assign(4 * (size_t)nSys * nn, 0.f); L.BLs.assign(4 * (size_t)nSys * nn, 0.f); L.BKs.assign(4 * (size_t)nSys * nn, 0.f);
     L.Ksp.assign(4 * (size_t)nSys * nn, 0.f); L.Kpp.assign(4 * (size_t)nSys * nn, 0.f);
     L.lvecs.assign(12 * (size_t)nSys, 0.f); L.ilvecs.assign(12 * (size_t)nSys, 0.f);
@@ -560,46 +571,74 @@ void optimizeLattice_1d(double* dlvec, int n1, int n2, int initMode, double tol)
 }
 void optimizeLattice_2d_multi(double* dlvec, int nstesp, int initMode, double tol) { optimizeLattice_1d(dlvec, 0, nstesp, initMode, tol); }
 
-// rigid placements (and optional relaxation) of the molecule: poss [nconf*3],
-// rots [nconf*9]; Es [nconf], aforces/aposs [nconf*natoms*3] (nullable)
+// MolWorld_sp3_multi::scan_relaxed (MolWorld_sp3_multi.h:1242-1296), which
+// MMFFmulti_lib.cpp:305-314 calls for every scan: configuration i is the
+// molecule placed by setFromRef (MMFFsp3_loc.h:1543-1551: p = rot^T ref +
+// poss[i], pi = rot^T pi_ref) with atom ipicked = 0 pinned to poss[i] by a unit
+// spring (constr / constrK), relaxed with niter_max FIRE steps to Fconv;
+// Es[i], aforces and aposs [nconf*natoms*3] (nullable) are its energy, forces
+// (without the spring) and positions afterwards.  The reference refills each
+// relaxed replica slot with the next configuration; here every configuration
+// is a system of one uploaded batch and the persistent relax kernels claim
+// them from their work queue, so a finished slot takes the next
+// configuration without a host round trip.  omp, bRelax, dt and Flim are not
+// used (as in the reference).  The replicas of init() are restored afterwards.
 void scan(int nconf, double* poss, double* rots, double* Es, double* aforces, double* aposs, bool omp, bool bRelax, int niter_max,
           double dt, double Fconv, double Flim) {
-    (void)omp; (void)dt; (void)Flim;
-    if (!L.ready) return;
+    (void)omp; (void)bRelax; (void)dt; (void)Flim;
+    if (!L.ready || nconf < 1 || !poss) return;
     const int na = L.mol.natoms, nn = L.mol.nnode, nv = na + nn;
-    V3 c{0, 0, 0};
-    for (int i = 0; i < na; i++) c = c + L.mol.pos[i];
-    c = c * (1.0 / na);
-    for (int c0 = 0; c0 < nconf; c0 += L.nSys) {
-        const int nb = std::min(L.nSys, nconf - c0);
-        for (int s = 0; s < L.nSys; s++) {
-            const int ic = c0 + std::min(s, nb - 1);
-            const double* R = rots + 9 * ic;
-            const V3 p0{poss[3 * ic], poss[3 * ic + 1], poss[3 * ic + 2]};
-            for (int v = 0; v < nv; v++) {
-                V3 d = (v < na) ? L.mol.pos[v] - c : L.mol.pos[v];
-                V3 r{R[0] * d.x + R[1] * d.y + R[2] * d.z, R[3] * d.x + R[4] * d.y + R[5] * d.z, R[6] * d.x + R[7] * d.y + R[8] * d.z};
-                if (v < na) r = r + p0;
-                L.atoms[4 * ((size_t)s * nv + v)] = (float)r.x; L.atoms[4 * ((size_t)s * nv + v) + 1] = (float)r.y; L.atoms[4 * ((size_t)s * nv + v) + 2] = (float)r.z;
-                for (int k = 0; k < 3; k++) L.avel[4 * ((size_t)s * nv + v) + k] = 0.f;
-            }
+    const int ipicked = 0;
+    std::vector<int> natoms(nconf, na), nnode(nconf, nn);
+    std::vector<double> pos(3 * (size_t)nconf * nv), ca(4 * (size_t)nconf * na, -1.0), ck(4 * (size_t)nconf * na, -1.0);
+    std::vector<int> ng(4 * (size_t)nconf * na), ngC(4 * (size_t)nconf * na), bk(4 * (size_t)nconf * na);
+    std::vector<double> REQ(4 * (size_t)nconf * na), ap(4 * (size_t)nconf * nn), bL(4 * (size_t)nconf * nn),
+        bK(4 * (size_t)nconf * nn), ks(4 * (size_t)nconf * nn), kp(4 * (size_t)nconf * nn), lv(9 * (size_t)nconf);
+    for (int c = 0; c < nconf; c++) {
+        static const double I3[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+        const double* R = rots ? rots + 9 * c : I3;
+        const V3 p0{poss[3 * c], poss[3 * c + 1], poss[3 * c + 2]};
+        for (int v = 0; v < nv; v++) {
+            const V3 d = L.mol.pos[v];
+            // Mat3d::dot_to_T: out_k = sum_j R[3 j + k] d_j
+            V3 r{R[0] * d.x + R[3] * d.y + R[6] * d.z, R[1] * d.x + R[4] * d.y + R[7] * d.z, R[2] * d.x + R[5] * d.y + R[8] * d.z};
+            if (v < na) r = r + p0;
+            pos[3 * ((size_t)c * nv + v)] = r.x; pos[3 * ((size_t)c * nv + v) + 1] = r.y; pos[3 * ((size_t)c * nv + v) + 2] = r.z;
         }
-        upload_all(false);
-        if (bRelax) mmff_relax(niter_max, Fconv, 0);
-        mmff_eval(1);
-        std::vector<double> E(4 * (size_t)L.nSys), F(3 * (size_t)L.nSys * nv), P(3 * (size_t)L.nSys * nv);
-        mmff_get_energies(E.data());
-        mmff_get_forces(F.data());
-        mmff_get_state(P.data(), nullptr, nullptr, nullptr, nullptr, nullptr);
-        for (int s = 0; s < nb; s++) {
-            const int ic = c0 + s;
-            if (Es) Es[ic] = E[4 * s + 3];
-            for (int a = 0; a < na; a++) for (int k = 0; k < 3; k++) {
-                if (aforces) aforces[3 * ((size_t)ic * na + a) + k] = F[3 * ((size_t)s * nv + a) + k];
-                if (aposs) aposs[3 * ((size_t)ic * na + a) + k] = P[3 * ((size_t)s * nv + a) + k];
-            }
+        const size_t ia = 4 * ((size_t)c * na + ipicked);
+        ca[ia] = p0.x; ca[ia + 1] = p0.y; ca[ia + 2] = p0.z; ca[ia + 3] = 1.0;
+        ck[ia] = ck[ia + 1] = ck[ia + 2] = ck[ia + 3] = 1.0;
+        // topology and parameters of replica 0
+        for (int a = 0; a < na; a++) for (int k = 0; k < 4; k++) {
+            ng[4 * ((size_t)c * na + a) + k] = L.gneighs[4 * (size_t)a + k];
+            ngC[4 * ((size_t)c * na + a) + k] = L.gneighCell[4 * (size_t)a + k];
+            bk[4 * ((size_t)c * na + a) + k] = L.gbkNeighs[4 * (size_t)a + k];
+            REQ[4 * ((size_t)c * na + a) + k] = L.REQs[4 * (size_t)a + k];
+        }
+        for (int i = 0; i < nn; i++) for (int k = 0; k < 4; k++) {
+            const size_t o = 4 * ((size_t)c * nn + i) + k, o0 = 4 * (size_t)i + k;
+            ap[o] = L.MMpars[o0]; bL[o] = L.BLs[o0]; bK[o] = L.BKs[o0]; ks[o] = L.Ksp[o0]; kp[o] = L.Kpp[o0];
+        }
+        for (int r = 0; r < 3; r++) for (int q = 0; q < 3; q++) lv[9 * c + 3 * r + q] = L.lvecs[4 * r + q];
+    }
+    auto check = [](int rc) { if (rc) set_error(std::string("scan: ") + mmff_last_error()); return rc != 0; };
+    if (check(mmff_systems_upload(nconf, natoms.data(), nnode.data(), pos.data(), nullptr, ng.data(), ngC.data(), bk.data(),
+                                  REQ.data(), ap.data(), bL.data(), bK.data(), ks.data(), kp.data(), lv.data())))
+        return;
+    if (check(mmff_set_constraints(ca.data(), ck.data())) || check(mmff_relax(niter_max, Fconv, 0)) || check(mmff_eval(1)))
+        return;
+    std::vector<double> E(4 * (size_t)nconf), F(3 * (size_t)nconf * nv), P(3 * (size_t)nconf * nv);
+    if (check(mmff_get_energies(E.data())) || check(mmff_get_forces(F.data())) ||
+        check(mmff_get_state(P.data(), nullptr, nullptr, nullptr, nullptr, nullptr)))
+        return;
+    for (int c = 0; c < nconf; c++) {
+        if (Es) Es[c] = E[4 * c + 3];
+        for (int a = 0; a < na; a++) for (int k = 0; k < 3; k++) {
+            if (aforces) aforces[3 * ((size_t)c * na + a) + k] = F[3 * ((size_t)c * nv + a) + k];
+            if (aposs) aposs[3 * ((size_t)c * na + a) + k] = P[3 * ((size_t)c * nv + a) + k];
         }
     }
+    check(upload_all(true));
 }
 
 // tri-state switches (>0 on, <0 off, 0 keep), MMFFmulti_lib.cpp:316-329

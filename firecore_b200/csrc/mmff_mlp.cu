@@ -564,6 +564,71 @@ __global__ void revert_kernel(Systems Y, const int* __restrict__ atom_sys, int N
     Y.pos[d.z + ga - d.x] = save[ga];
 }
 
+// Rigid-body projection of the proposal, one warp per system: the translation
+// t and rotation vector w that best reproduce the per-atom displacements d_i
+// in least squares (minimise sum |d_i - t - w x u_i|^2, u_i = p_i - centroid:
+// t = mean d, (sum |u|^2 1 - u u^T) w = sum u x (d - t), FP64), then d_i is
+// replaced by t + (R(w) - 1) u_i with R the rotation by |w| about w (Rodrigues).
+// A rigid move keeps every bond, angle and pi term of the molecule, so the
+// energy gate only weighs the molecule's placement against the substrate and
+// its own images: the network's per-atom outputs act as a vote on one
+// translation and one rotation per molecule.
+__global__ void rigid_kernel(Systems Y, int nsys, const float4* __restrict__ save, float4* __restrict__ disp) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (w >= nsys) return;                      // whole warps
+    const int4 d = Y.desc[w];
+    const int a0 = d.x, n = d.w;
+    auto red = [](double v) {
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        return v;
+    };
+    double c[3] = {0, 0, 0}, t[3] = {0, 0, 0};
+    for (int i = lane; i < n; i += 32) {
+        const float4 p = save[a0 + i], q = disp[a0 + i];
+        c[0] += p.x; c[1] += p.y; c[2] += p.z; t[0] += q.x; t[1] += q.y; t[2] += q.z;
+    }
+    for (int k = 0; k < 3; k++) { c[k] = red(c[k]) / n; t[k] = red(t[k]) / n; }
+    double A[6] = {0, 0, 0, 0, 0, 0}, b[3] = {0, 0, 0};     // xx yy zz xy xz yz
+    for (int i = lane; i < n; i += 32) {
+        const float4 p = save[a0 + i], q = disp[a0 + i];
+        const double u0 = p.x - c[0], u1 = p.y - c[1], u2 = p.z - c[2];
+        const double e0 = q.x - t[0], e1 = q.y - t[1], e2 = q.z - t[2];
+        const double uu = u0 * u0 + u1 * u1 + u2 * u2;
+        A[0] += uu - u0 * u0; A[1] += uu - u1 * u1; A[2] += uu - u2 * u2;
+        A[3] -= u0 * u1; A[4] -= u0 * u2; A[5] -= u1 * u2;
+        b[0] += u1 * e2 - u2 * e1; b[1] += u2 * e0 - u0 * e2; b[2] += u0 * e1 - u1 * e0;
+    }
+    for (int k = 0; k < 6; k++) A[k] = red(A[k]);
+    for (int k = 0; k < 3; k++) b[k] = red(b[k]);
+    const double tr = A[0] + A[1] + A[2];
+    for (int k = 0; k < 3; k++) A[k] += 1e-9 * tr + 1e-12;       // collinear / single-atom systems
+    // symmetric 3x3 solve by the adjugate
+    const double c00 = A[1] * A[2] - A[5] * A[5], c01 = A[4] * A[5] - A[3] * A[2], c02 = A[3] * A[5] - A[4] * A[1];
+    const double c11 = A[0] * A[2] - A[4] * A[4], c12 = A[3] * A[4] - A[0] * A[5], c22 = A[0] * A[1] - A[3] * A[3];
+    const double det = A[0] * c00 + A[3] * c01 + A[4] * c02;
+    double om[3] = {0, 0, 0};
+    if (det > 0) {
+        om[0] = (c00 * b[0] + c01 * b[1] + c02 * b[2]) / det;
+        om[1] = (c01 * b[0] + c11 * b[1] + c12 * b[2]) / det;
+        om[2] = (c02 * b[0] + c12 * b[1] + c22 * b[2]) / det;
+    }
+    const double th = sqrt(om[0] * om[0] + om[1] * om[1] + om[2] * om[2]);
+    double R[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    if (th > 1e-12) {
+        const double x = om[0] / th, y = om[1] / th, z = om[2] / th, cs = cos(th), sn = sin(th), cc = 1 - cs;
+        R[0] = cs + x * x * cc;     R[1] = x * y * cc - z * sn; R[2] = x * z * cc + y * sn;
+        R[3] = y * x * cc + z * sn; R[4] = cs + y * y * cc;     R[5] = y * z * cc - x * sn;
+        R[6] = z * x * cc - y * sn; R[7] = z * y * cc + x * sn; R[8] = cs + z * z * cc;
+    }
+    for (int i = lane; i < n; i += 32) {
+        const float4 p = save[a0 + i];
+        const double u0 = p.x - c[0], u1 = p.y - c[1], u2 = p.z - c[2];
+        disp[a0 + i] = make_float4((float)(t[0] + R[0] * u0 + R[1] * u1 + R[2] * u2 - u0),
+                                   (float)(t[1] + R[3] * u0 + R[4] * u1 + R[5] * u2 - u1),
+                                   (float)(t[2] + R[6] * u0 + R[7] * u1 + R[8] * u2 - u2), 0.f);
+    }
+}
+
 }  // namespace mlp
 }  // namespace mmff
 
@@ -600,6 +665,7 @@ struct Net {
     Buf<int> err, atom_sys, elem, accepted, keep;
     float out_scale = 1.f;
     int ndata = 0, ntile_data = 0, na_elem = 0;
+    int projection = 0;                     // warm start: 0 per-atom moves, 1 rigid-body projection
     bool attr_set = false;
 };
 Net N;
@@ -874,6 +940,40 @@ int mmff_mlp_features(double z_top, float* out) {
     return 0;
 }
 
+// How warm-start moves use the network's per-atom displacements: 0 as they
+// are, 1 projected on one rigid-body move per system (rigid_kernel).
+int mmff_mlp_set_projection(int mode) {
+    if (mode != 0 && mode != 1) return fail("mmff_mlp_set_projection: mode must be 0 or 1");
+    N.projection = mode;
+    return 0;
+}
+
+// The rigid-body projection of displacements disp [NA][3] (host, FP64) at the
+// systems' current positions -> out [NA][3]: the kernel the warm start uses,
+// for checks against a restatement.
+int mmff_mlp_project(const double* disp, double* out) {
+    WorldView V;
+    if (world_view(&V)) return -1;
+    if (!disp || !out) return fail("mmff_mlp_project: NULL array");
+    if (N.outs.ensure(V.NA) || N.save.ensure(V.NA) || N.atom_sys.ensure(V.NA)) return -1;
+    std::vector<int> as(V.NA);
+    for (int s = 0; s < V.nsys; s++)
+        for (int i = 0; i < V.desc[s].w; i++) as[V.desc[s].x + i] = s;
+    std::vector<float4> h(V.NA);
+    for (int i = 0; i < V.NA; i++) h[i] = make_float4((float)disp[3 * i], (float)disp[3 * i + 1], (float)disp[3 * i + 2], 0.f);
+    MCK(cudaMemcpyAsync(N.atom_sys.p, as.data(), V.NA * sizeof(int), cudaMemcpyHostToDevice, V.stream));
+    MCK(cudaMemcpyAsync(N.outs.p, h.data(), V.NA * sizeof(float4), cudaMemcpyHostToDevice, V.stream));
+    const unsigned ga = (V.NA + 255) / 256;
+    save_kernel<<<ga, 256, 0, V.stream>>>(V.Y, N.atom_sys.p, V.NA, N.save.p);
+    rigid_kernel<<<(unsigned)((V.nsys + 3) / 4), 128, 0, V.stream>>>(V.Y, V.nsys, N.save.p, N.outs.p);
+    mmff_count_launches(2);
+    MCK(cudaGetLastError());
+    MCK(cudaMemcpyAsync(h.data(), N.outs.p, V.NA * sizeof(float4), cudaMemcpyDeviceToHost, V.stream));
+    MCK(cudaStreamSynchronize(V.stream));
+    for (int i = 0; i < V.NA; i++) { out[3 * i] = h[i].x; out[3 * i + 1] = h[i].y; out[3 * i + 2] = h[i].z; }
+    return 0;
+}
+
 int mmff_mlp_warmstart(int nsteps, double z_top, int* accepted) {
     if (need_params()) return -1;
     WorldView V;
@@ -894,6 +994,10 @@ int mmff_mlp_warmstart(int nsteps, double z_top, int* accepted) {
         if (run_net(false, N.Xs.p, nullptr, ntile, V.NA, 0.f, N.outs.p, V.stream)) return -1;
         save_kernel<<<ga, 256, 0, V.stream>>>(V.Y, N.atom_sys.p, V.NA, N.save.p);
         mmff_count_launches(1);
+        if (N.projection == 1) {
+            rigid_kernel<<<(unsigned)((V.nsys + 3) / 4), 128, 0, V.stream>>>(V.Y, V.nsys, N.save.p, N.outs.p);
+            mmff_count_launches(1);
+        }
         MCK(cudaMemsetAsync(N.keep.p, 0, V.nsys * sizeof(int), V.stream));
         // step-length search along the proposal: the first length that lowers
         // a system's energy is kept, otherwise the system stays where it was

@@ -600,11 +600,20 @@ struct Engine {
             return;
         }
         const int nunits = natoms * 4;
+        const bool cached = Y.gkey != nullptr;      // launch-uniform
         for (int u0 = 0; u0 < nunits; u0 += nt) {
             const int u = u0 + t0;
             const int i = u >> 2, a = u & 3;
             float4 r = make_float4(0, 0, 0, 0);
-            if (i < natoms) {
+            if (cached) {
+                const bool ok = i < natoms;
+                const int ic = ok ? i : natoms - 1;
+                const float4 p = spos[ic];
+                const float3 uu = make_float3((p.x + gorg.x) * P.ginv[0], (p.y + gorg.y) * P.ginv[1],
+                                              (p.z + gorg.z) * P.ginv[2]);
+                r = grid_slice_cached<(T >= MMFF_UNROLL_MIN_T) ? 4 : 1>(P.grid, P.gn[0], P.gn[1], P.gn[2], uu, plq(ic),
+                                                                       a, ok, Y.gkey, Y.gcs, aoff + ic);
+            } else if (i < natoms) {
                 const float4 p = spos[i];
                 const float3 uu = make_float3((p.x + gorg.x) * P.ginv[0], (p.y + gorg.y) * P.ginv[1],
                                               (p.z + gorg.z) * P.ginv[2]);
@@ -805,6 +814,10 @@ struct Engine {
                 const float fr2 = dot3(f, f);
                 if (fr2 > Fl2) f = f * (P.Flim * rsqrtf(fr2));
             }
+            if ((P.flags & F_CONSTR) && v < natoms) f = constraint_force(Y, aoff + v, f3(spos[v]), f);
+            // a system whose atoms left any sensible range (no force clamp,
+            // bad start) is retired like a non-finite one
+            if (v < natoms) { const float4 p = spos[v]; bad |= !(fabsf(p.x) + fabsf(p.y) + fabsf(p.z) < 1e5f); }
             fasm[v] = make_float4(f.x, f.y, f.z, 0.f);
             const float4 vv4 = svel[v];
             vf += (double)vv4.x * f.x + (double)vv4.y * f.y + (double)vv4.z * f.z;

@@ -578,6 +578,9 @@ struct WarpEngine {
                     const float fr2 = dot3(f, f);
                     if (fr2 > Fl * Fl) f = f * (Fl * rsqrtf(fr2));
                 }
+                if ((P.flags & F_CONSTR) && w == 0) f = constraint_force(Y, aoff + a, f3(sp[a]), f);
+                // a system whose atoms left any sensible range is retired like a non-finite one
+                if (w == 0) { const float4 p = sp[a]; b |= !(fabsf(p.x) + fabsf(p.y) + fabsf(p.z) < 1e5f); }
                 if (w == 0) fasm_a[k] = f; else fasm_p[k] = f;
                 vf += (double)v.x * f.x + (double)v.y * f.y + (double)v.z * f.z;
                 vv += (double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z;

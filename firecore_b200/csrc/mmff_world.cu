@@ -110,6 +110,12 @@ struct World {
     std::vector<int> h_a13;
     DBuf<int> d_a13, d_moff;
     DBuf<uint32_t> d_xmask;
+    // position springs (relax only)
+    DBuf<float4> d_constr, d_constrK;
+    bool has_constr = false;
+    // per-atom GridFF stencil cache of the CTA engine (grid_slice_cached)
+    DBuf<unsigned int> d_gkey; DBuf<float4> d_gcs;
+    bool gcache = true;            // mmff_set_grid_cache
     DBuf<float4> d_pos, d_vel, d_force, d_pos0, d_vel0;
     DBuf<double4> d_fire, d_fire0, d_energy;
     DBuf<int> d_status, d_nsteps, d_counter;
@@ -165,6 +171,8 @@ Params make_params(bool for_eval, int nstep_max, double Fconv, int conv_mode) {
     memset(&P, 0, sizeof P);
     P.flags = W.flags & ~F_EXCL13;
     if (excl13_active(P.flags)) P.flags |= F_EXCL13;
+    P.flags &= ~F_CONSTR;
+    if (W.has_constr && !for_eval) P.flags |= F_CONSTR;
     if (!W.grid.p) P.flags &= ~F_GRID;
     for (int k = 0; k < 3; k++) P.npbc[k] = W.npbc[k];
     P.Rc2 = W.Rcut > 0 ? (float)(W.Rcut * W.Rcut) : 0.f;
@@ -202,6 +210,10 @@ Systems make_systems() {
     Y.REQ = W.d_REQ.p; Y.PLQ = W.d_PLQ.p; Y.neighs = W.d_ng.p; Y.neighCell = W.d_ngC.p; Y.bkneighs = W.d_bk.p;
     Y.apars = W.d_apar.p; Y.bLs = W.d_bL.p; Y.bKs = W.d_bK.p; Y.Ksp = W.d_ksp.p; Y.Kpp = W.d_kpp.p;
     Y.a13 = W.d_a13.p; Y.xmask = W.d_xmask.p; Y.moff = W.d_moff.p;
+    Y.constr = W.d_constr.p; Y.constrK = W.d_constrK.p;
+    // the cache keys pack the stencil cell into 12 + 12 + 8 bits
+    const bool gc = W.gcache && W.d_gkey.p && W.gn[0] <= 4096 && W.gn[1] <= 4096 && W.gn[2] <= 256;
+    Y.gkey = gc ? W.d_gkey.p : nullptr; Y.gcs = gc ? W.d_gcs.p : nullptr;
     Y.pos = W.d_pos.p; Y.vel = W.d_vel.p; Y.force = W.d_force.p; Y.fire = W.d_fire.p;
     Y.status = W.d_status.p; Y.nsteps = W.d_nsteps.p; Y.fconv = W.d_fconv.p; Y.energy = W.d_energy.p;
     Y.counters = W.d_stats.p;
@@ -290,6 +302,12 @@ void default_config(int cls, int maxNA, int& kind, int& apl, int& T, int& S) {
 template <class X> int upload(DBuf<X>& d, const std::vector<X>& h) {
     if (d.ensure(h.size())) return -1;
     if (!h.empty()) CK(cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(X), cudaMemcpyHostToDevice, W.stream));
+    return 0;
+}
+
+// Empty every atom's GridFF stencil cache (new systems, new grid).
+int clear_grid_cache() {
+    if (W.d_gkey.p && W.NA > 0) CK(cudaMemsetAsync(W.d_gkey.p, 0xff, (size_t)W.NA * sizeof(unsigned int), W.stream));
     return 0;
 }
 
@@ -512,6 +530,14 @@ int mmff_set_fire(double dt_max, double dt_min, double damp_max, double finc, do
     return 0;
 }
 
+// Per-atom GridFF stencil cache of the CTA relax kernels on (default) or off
+// (every step gathers the 64 grid coefficients); results are bit-identical.
+int mmff_set_grid_cache(int on) {
+    W.version++;
+    W.gcache = on != 0;
+    return clear_grid_cache();
+}
+
 int mmff_set_launch(int threads, int pair_split) {
     if (threads && threads != 64 && threads != 128 && threads != 256 && threads != 512) return fail("threads must be 64/128/256/512");
     if (pair_split && pair_split != 1 && pair_split != 2 && pair_split != 4 && pair_split != 8) return fail("pair_split must be 1/2/4/8");
@@ -528,6 +554,7 @@ int mmff_grid_upload(int nx, int ny, int nz, const double* pos0, const double* s
     for (size_t i = 0; i < n; i++) h[i] = make_float4((float)coefs[3 * i], (float)coefs[3 * i + 1], (float)coefs[3 * i + 2], 0.f);
     if (W.grid.ensure(n)) return -1;
     CK(cudaMemcpyAsync(W.grid.p, h.data(), n * sizeof(float4), cudaMemcpyHostToDevice, W.stream));
+    if (clear_grid_cache()) return -1;
     CK(cudaStreamSynchronize(W.stream));
     W.gn[0] = nx; W.gn[1] = ny; W.gn[2] = nz;
     for (int k = 0; k < 3; k++) { W.gpos0[k] = pos0[k]; W.gstep[k] = step[k]; }
@@ -578,6 +605,7 @@ int mmff_grid_build(int nsub, const double* spos, const double* sREQ, const doub
     pack_grid_kernel<<<(unsigned)((ntot + 255) / 256), 256, 0, W.stream>>>(ntot, V.p, W.grid.p);
     CK(cudaGetLastError());
     if (coefs_out) CK(cudaMemcpyAsync(coefs_out, V.p, 3 * ntot * sizeof(double), cudaMemcpyDeviceToHost, W.stream));
+    if (clear_grid_cache()) return -1;
     CK(cudaStreamSynchronize(W.stream));
     W.gn[0] = nx; W.gn[1] = ny; W.gn[2] = nz;
     for (int k = 0; k < 3; k++) { W.gpos0[k] = pos0[k]; W.gstep[k] = step[k]; }
@@ -661,13 +689,45 @@ int mmff_systems_upload(int nsys, const int* natoms, const int* nnode, const dou
         upload(W.d_a13, ha13))
         return -1;
     W.h_ng = std::move(hng); W.h_ngC = std::move(hngC); W.h_a13 = std::move(ha13);
+    W.has_constr = false;           // springs belong to the systems they were set for
     if (W.d_force.ensure(NV) || W.d_energy.ensure(nsys) || W.d_status.ensure(nsys) || W.d_nsteps.ensure(nsys) ||
-        W.d_fconv.ensure(nsys) || W.d_counter.ensure(64) || W.d_stats.ensure(8))
+        W.d_fconv.ensure(nsys) || W.d_counter.ensure(64) || W.d_stats.ensure(8) || W.d_gkey.ensure(NA) ||
+        W.d_gcs.ensure((size_t)NA * 16) || clear_grid_cache())
         return -1;
     CK(cudaMemsetAsync(W.d_status.p, 0, nsys * sizeof(int), W.stream));
     CK(cudaMemsetAsync(W.d_nsteps.p, 0, nsys * sizeof(int), W.stream));
     CK(cudaStreamSynchronize(W.stream));
     W.buckets_dirty = true;
+    return 0;
+}
+
+// Position springs of the uploaded systems (relax_multi.cl:995-1010): per atom
+// anchor [sum natoms][4] = (x, y, z) in world coordinates and w > 0 to switch
+// the spring on, constants K [sum natoms][4] = (kx, ky, kz, -); the relax
+// kernels add (anchor - p) * max(K, 0) to the atom's force after the clamp.
+// NULL anchor clears them.  Uploading systems clears them too.
+int mmff_set_constraints(const double* anchor, const double* K) {
+    if (ensure_ready()) return -1;
+    if (!W.nsys) return fail("no systems uploaded");
+    W.version++;
+    if (!anchor) { W.has_constr = false; return 0; }
+    if (!K) return fail("mmff_set_constraints: K is NULL");
+    std::vector<float4> ha(W.NA), hk(W.NA);
+    bool any = false;
+    for (int s = 0; s < W.nsys; s++) {
+        const int a0 = W.desc[s].x;
+        const double* o = W.orig.data() + 3 * s;
+        for (int i = 0; i < W.natoms[s]; i++) {
+            const double* c = anchor + 4 * (a0 + i);
+            const double* k = K + 4 * (a0 + i);
+            ha[a0 + i] = make_float4((float)(c[0] - o[0]), (float)(c[1] - o[1]), (float)(c[2] - o[2]), c[3] > 0 ? 1.f : -1.f);
+            hk[a0 + i] = make_float4((float)k[0], (float)k[1], (float)k[2], 0.f);
+            any |= c[3] > 0;
+        }
+    }
+    if (upload(W.d_constr, ha) || upload(W.d_constrK, hk)) return -1;
+    CK(cudaStreamSynchronize(W.stream));
+    W.has_constr = any;
     return 0;
 }
 

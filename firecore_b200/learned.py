@@ -110,6 +110,18 @@ class Proposal:
         _check(self.lib.mmff_mlp_features(z_top, _lib.ptr(out)), "mmff_mlp_features")
         return out
 
+    def set_projection(self, mode: int):
+        """0: warm-start moves are the per-atom displacements; 1: their rigid-body
+        projection per system (one translation + rotation per molecule)."""
+        _check(self.lib.mmff_mlp_set_projection(int(mode)), "mmff_mlp_set_projection")
+
+    def project(self, disp) -> np.ndarray:
+        """Rigid-body projection [sum natoms, 3] of displacements at the current positions."""
+        d = np.ascontiguousarray(disp, np.float64)
+        out = np.zeros_like(d)
+        _check(self.lib.mmff_mlp_project(_lib.ptr(d), _lib.ptr(out)), "mmff_mlp_project")
+        return out
+
     def warmstart(self, nsys: int, nsteps: int = 2, z_top: float = 0.0) -> np.ndarray:
         acc = np.zeros(nsys, np.int32)
         _check(self.lib.mmff_mlp_warmstart(nsteps, z_top, _lib.ptr(acc)), "mmff_mlp_warmstart")

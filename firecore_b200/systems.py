@@ -2,7 +2,8 @@
 
 Molecules: heavy-atom trees with C:N:O:H = 10:2:2:10, heavy-heavy bonds
 1.40 +- 0.05 A, X-H caps 1.09 A, angle / pi terms by hybridisation, charges
-N(0, 0.2) e re-centred to zero net (native generator ``mmff_gen_systems``).
+N(0, 0.2) e re-centred to zero net (native generator ``mmff_gen_systems`` of the
+host-only ``libmmff_gen.so``).
 Substrate: rigid rock-salt (001) slab, a = 5.64 A, 3 layers, 4 x 4 cells,
 ions +-0.9 e, periodic in x, y.
 
@@ -76,7 +77,7 @@ def make_systems(natoms: Sequence[int], seed: int, topo_mode: int = 1, sigma: fl
                  rotate: bool = True, zplace: float = 3.0, cell=(22.56, 22.56, 40.0),
                  hbond: bool = False, npbc=(1, 1, 0)) -> SystemBatch:
     """Generate ``len(natoms)`` seeded molecules (see module docstring)."""
-    lib = _lib.load()
+    lib = _lib.gen()
     natoms = np.ascontiguousarray(natoms, dtype=np.int32)
     nsys = natoms.shape[0]
     nnode = np.array([lib.mmff_gen_nnode(int(n)) for n in natoms], np.int32)
@@ -127,7 +128,7 @@ def make_slab(a: float = 5.64, ncell: int = 4, layers: int = 3, q: float = 0.9, 
     The x, y grid spacing is the cell edge divided by round(L / grid_step), so the
     grid is commensurate with the periodic cell; z starts ``z0`` above the top
     layer (no grid node sits on an ion)."""
-    lib = _lib.load()
+    lib = _lib.gen()
     nsub = 4 * ncell * ncell * layers
     spos = np.zeros((nsub, 3)); sREQ = np.zeros((nsub, 4))
     rc = np.array(REQ_cation, np.float64); ra = np.array(REQ_anion, np.float64)

@@ -70,6 +70,10 @@ class World:
     def set_launch(self, threads=0, pair_split=0):
         _check(self.lib.mmff_set_launch(threads, pair_split), "mmff_set_launch")
 
+    def set_grid_cache(self, on: bool = True):
+        """Per-atom GridFF stencil cache of the CTA relax kernels (bit-identical results)."""
+        _check(self.lib.mmff_set_grid_cache(int(on)), "mmff_set_grid_cache")
+
     def set_graph(self, on: bool = True):
         """Replay mmff_relax as one captured CUDA graph per parameter set."""
         _check(self.lib.mmff_set_graph(int(on)), "mmff_set_graph")
@@ -152,6 +156,17 @@ class World:
                                             _lib.ptr(a["bLs"]), _lib.ptr(a["bKs"]), _lib.ptr(a["Ksp"]),
                                             _lib.ptr(a["Kpp"]), _lib.ptr(a["lvec"])), "mmff_systems_upload")
         self.batch = b
+
+    def set_constraints(self, anchor=None, K=None):
+        """Per-atom position springs for relaxations (relax_multi.cl:995-1010):
+        anchor [sum natoms, 4] = (x, y, z, on if > 0) in world coordinates,
+        K [sum natoms, 3 or 4] spring constants; None clears."""
+        if anchor is None:
+            _check(self.lib.mmff_set_constraints(None, None), "mmff_set_constraints")
+            return
+        a = np.ascontiguousarray(anchor, np.float64)
+        k = np.zeros((a.shape[0], 4)); k[:, :np.asarray(K).shape[1]] = K
+        _check(self.lib.mmff_set_constraints(_lib.ptr(a), _lib.ptr(k)), "mmff_set_constraints")
 
     def restore(self):
         _check(self.lib.mmff_systems_restore(), "mmff_systems_restore")

@@ -108,6 +108,20 @@ int mmff_systems_upload(int nsys, const int* natoms, const int* nnode, const dou
                         const int* neighs, const int* neighCell, const int* bkneighs, const double* REQs,
                         const double* apars, const double* bLs, const double* bKs, const double* Ksp,
                         const double* Kpp, const double* lvec);
+/* Per-atom position springs for relaxations (the constr / constrK buffers
+ * of updateAtomsMMFFf4, relax_multi.cl:995-1010; MolWorld_sp3_multi.h:
+ * 1270-1273 sets them for scan_relaxed): anchor [sum natoms][4] = (x, y, z)
+ * world coordinates and w > 0 to switch the spring on, K [sum natoms][4] =
+ * (kx, ky, kz, -); the relax kernels add (anchor - p) * max(K, 0) to the
+ * atom's force after the force clamp.  mmff_eval reports forces without
+ * them.  anchor NULL clears; mmff_systems_upload clears. */
+int mmff_set_constraints(const double* anchor, const double* K);
+/* No counterpart in the reference.  Per-atom cache of the 64 channel-combined
+ * B-spline coefficients (PLQ . C) of the atom's GridFF stencil in the CTA
+ * relax kernels: on (1, default) an atom re-gathers the grid only when its
+ * stencil cell changes; off (0) every step gathers.  Results are
+ * bit-identical either way; 260 B of device memory per atom. */
+int mmff_set_grid_cache(int on);
 /* Restore positions, velocities and FIRE state saved at upload (device copy). */
 int mmff_systems_restore(void);
 /* Overwrite positions (and velocities; NULL = 0); reset_fire != 0 resets dt,
@@ -310,6 +324,15 @@ int mmff_mlp_train(int nsteps, int batch_tiles, double lr, double wd, double* lo
 int mmff_mlp_set_elements(const int* elem);
 /* Raw descriptors [sum natoms][68] of the current positions; z_top = slab top [A]. */
 int mmff_mlp_features(double z_top, float* out);
+/* No counterpart in the reference.  How warm-start moves use the network's
+ * per-atom displacements: 0 as they are (default), 1 projected per system on
+ * the least-squares rigid-body move (translation + rotation, FP64 fit), which
+ * leaves every bonded term of the molecule unchanged. */
+int mmff_mlp_set_projection(int mode);
+/* No counterpart in the reference.  That rigid-body projection of host
+ * displacements disp [sum natoms][3] at the systems' current positions ->
+ * out [sum natoms][3] (the warm start's kernel, for checks). */
+int mmff_mlp_project(const double* disp, double* out);
 /* nsteps learned moves on every system: descriptors -> network proposal d ->
  * trial positions x + a d for a = 1, 1/2, 1/4, 1/8 -> the first trial that
  * lowers the system's total energy is kept, else the system stays at x;

@@ -159,3 +159,32 @@ def adamw(p, g, m, v, t, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8, wd=0.01):
     out["W3"][NOUT:] = 0.0
     out["b3"][NOUT:] = 0.0
     return out
+
+
+def rigid_projection(pos, disp, natoms):
+    """Rigid-body projection of per-atom displacements, per system (the warm
+    start's projection, restated in FP64): t = mean d; w solves
+    (sum |u|^2 1 - u u^T) w = sum u x (d - t) with u = p - centroid; the
+    projected displacement is t + (R(w) - 1) u, R the rotation by |w| about w.
+    pos, disp [sum natoms, 3]; natoms [nsys]."""
+    out = np.zeros_like(disp, dtype=np.float64)
+    o = 0
+    for n in natoms:
+        p = np.asarray(pos[o:o + n], np.float64)
+        d = np.asarray(disp[o:o + n], np.float64)
+        u = p - p.mean(0)
+        t = d.mean(0)
+        e = d - t
+        A = np.eye(3) * (u * u).sum() - u.T @ u
+        A += np.eye(3) * (1e-9 * np.trace(A) + 1e-12)
+        b = np.cross(u, e).sum(0)
+        w = np.linalg.solve(A, b) if np.linalg.det(A) > 0 else np.zeros(3)
+        th = np.linalg.norm(w)
+        R = np.eye(3)
+        if th > 1e-12:
+            k = w / th
+            K = np.array([[0, -k[2], k[1]], [k[2], 0, -k[0]], [-k[1], k[0], 0]])
+            R = np.eye(3) + np.sin(th) * K + (1 - np.cos(th)) * K @ K
+        out[o:o + n] = t + u @ R.T - u
+        o += n
+    return out

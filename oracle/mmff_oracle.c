@@ -519,7 +519,8 @@ void orc_relax(int nsys, const int* natoms, const int* nnode,
                const double* bKs, const double* Ksp, const double* Kpp,
                const double* lvec, const double* gridC, const ORC_params* P,
                const ORC_fire* F, int niter, double Fconv, int conv_mode,
-               int* nsteps_out, int* conv_out, double* Fout, double* Eout, int nthreads) {
+               int* nsteps_out, int* conv_out, double* Fout, double* Eout, int nthreads,
+               const double* constr, const double* constrK) {
     offsets_t o = make_offsets(nsys, natoms, nnode);
     size_t nvtot = (size_t)o.voff[nsys];
     double* force = (double*)calloc(nvtot * 3 + 3, sizeof(double));
@@ -550,6 +551,20 @@ void orc_relax(int nsys, const int* natoms, const int* nnode,
                     double* fi = S.force + 3 * i;
                     double fr2 = fi[0] * fi[0] + fi[1] * fi[1] + fi[2] * fi[2];
                     if (fr2 > Fl2) { double c = F->Flim / sqrt(fr2); fi[0] *= c; fi[1] *= c; fi[2] *= c; }
+                }
+            }
+            /* position springs of updateAtomsMMFFf4 (relax_multi.cl:995-1010):
+             * after the clamp, atoms only, (anchor - p) * max(K, 0) where anchor.w > 0 */
+            if (constr) {
+                const double* cs = constr + 4 * o.aoff[s];
+                const double* ck = constrK + 4 * o.aoff[s];
+                for (int i = 0; i < S.natoms; i++) {
+                    if (!(cs[4 * i + 3] > 0)) continue;
+                    double* fi = S.force + 3 * i;
+                    for (int k = 0; k < 3; k++) {
+                        const double kk = ck[4 * i + k] > 0 ? ck[4 * i + k] : 0.0;
+                        fi[k] += (cs[4 * i + k] - p[3 * i + k]) * kk;
+                    }
                 }
             }
             double vf = 0, vv = 0, ff = 0, fmax2 = 0;

@@ -95,7 +95,7 @@ void orc_relax(int nsys, const int* natoms, const int* nnode,
                const double* lvec, const double* gridC, const ORC_params* P,
                const ORC_fire* F, int niter, double Fconv, int conv_mode,
                int* nsteps_out, int* conv_out, double* Fout, double* Eout,
-               int nthreads);
+               int nthreads, const double* constr, const double* constrK);
 
 /* Langevin dynamics, MMFFsp3_loc::move_atom_Langevin (MMFFsp3_loc.h:1191-1216):
  * per step and vector f -= gamma v; f += u sqrt(2 kB T gamma / dt) with u in

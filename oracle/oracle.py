@@ -146,8 +146,11 @@ def eval_forces(b, P: ORCParams, gridC=None, pos=None, nthreads=0):
 
 
 def relax(b, P: ORCParams, F: ORCFire, gridC=None, niter=1000, Fconv=1e-4, conv_mode=0, pos=None, vel=None,
-          fire_state=None, nthreads=0):
-    """FIRE relaxation (run_no_omp semantics). Returns dict of arrays."""
+          fire_state=None, nthreads=0, constr=None, constrK=None):
+    """FIRE relaxation (run_no_omp semantics). Returns dict of arrays.
+    constr / constrK [sum natoms, 4] (optional): per-atom position springs,
+    anchor (x, y, z, on if w > 0) and constants (kx, ky, kz, -) in the same
+    frame as pos."""
     lib = orc()
     pos = np.array(b.pos if pos is None else pos, np.float64, order="C")
     vel = np.zeros_like(pos) if vel is None else np.array(vel, np.float64, order="C")
@@ -161,9 +164,12 @@ def relax(b, P: ORCParams, F: ORCFire, gridC=None, niter=1000, Fconv=1e-4, conv_
     keep = [np.ascontiguousarray(b.natoms, np.int32), np.ascontiguousarray(b.nnode, np.int32)]
     g = None if gridC is None else np.ascontiguousarray(gridC, np.float64)
     arrs = _sysarrays(b)
+    cs = None if constr is None else np.ascontiguousarray(constr, np.float64)
+    ck = None if constrK is None else np.ascontiguousarray(constrK, np.float64)
     lib.orc_relax(ctypes.c_int(b.nsys), _p(keep[0]), _p(keep[1]), _p(pos), _p(vel), _p(fire_state), *[_p(a) for a in arrs],
                   _p(g), ctypes.byref(P), ctypes.byref(F), ctypes.c_int(niter), ctypes.c_double(Fconv),
-                  ctypes.c_int(conv_mode), _p(nsteps), _p(conv), _p(Fout), _p(Eout), ctypes.c_int(nthreads))
+                  ctypes.c_int(conv_mode), _p(nsteps), _p(conv), _p(Fout), _p(Eout), ctypes.c_int(nthreads),
+                  _p(cs), _p(ck))
     return dict(pos=pos, vel=vel, fire_state=fire_state, nsteps=nsteps, converged=conv, F=Fout, E=Eout)
 
 

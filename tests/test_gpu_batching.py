@@ -52,6 +52,28 @@ def test_graph_relax_is_identical_to_direct_launches(world, golden):
     world.set_graph(False)
 
 
+def test_grid_cache_is_bit_identical(world, golden):
+    """The per-atom GridFF stencil cache of the CTA kernels changes no bit:
+    a relaxation (cells change every few steps early on, rarely later) and an
+    evaluation with the cache on and off; also after a restore, where every
+    cached cell is stale."""
+    b = uneven(world, golden, n=64, seed=9, lo=40, hi=300)
+    world.set_launch(128, 0)                 # CTA engine for every size
+    out = {}
+    for on in (False, True, True):
+        world.set_grid_cache(on)
+        world.restore(); world.relax(400, 1e-4, conv_mode=1)
+        st = world.state()
+        F, E = world.eval(True)
+        out.setdefault(on, []).append((st, F, E))
+    world.set_grid_cache(True)
+    world.set_launch(0, 0)
+    (d, Fd, Ed), = out[False]
+    for g, Fg, Eg in out[True]:
+        assert np.array_equal(d["pos"], g["pos"]) and np.array_equal(d["nsteps"], g["nsteps"])
+        assert np.array_equal(Fd, Fg) and np.array_equal(Ed, Eg)
+
+
 def test_autotune_picks_a_launchable_config_and_keeps_physics(world, golden, tmp_path):
     b = uneven(world, golden)
     for c in range(6):

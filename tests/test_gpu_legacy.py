@@ -32,10 +32,18 @@ def test_legacy_init_run_eval_scan(tmp_path):
     E = mmff.eval()
     assert np.isfinite(E)
     assert np.allclose(mmff.Es[0], E)
-    # rigid scan of the molecule over 3 heights
-    poss = np.array([[5.6, 5.6, z] for z in (6.0, 7.0, 8.0)])
-    Es, _, _ = mmff.scan(poss, bRelax=False)
-    assert np.isfinite(Es).all()
+    # scan_relaxed (MolWorld_sp3_multi.h:1242-1296): 5 placements, atom 0 pinned
+    # to each target by a unit spring, every configuration relaxed on the queue
+    poss = np.array([[5.6, 5.6, z] for z in (6.0, 6.5, 7.0, 7.5, 8.0)])
+    Es, aforces, aposs = mmff.scan(poss, bF=True, bP=True, bRelax=True, niter_max=4000, Fconv=1e-3)
+    assert np.isfinite(Es).all() and np.isfinite(aforces).all()
+    assert aposs.shape == (5, 24, 3)
+    # the pinned atom stays near its target (spring force = the net other force)
+    d = np.linalg.norm(aposs[:, 0, :] - poss, axis=1)
+    assert d.max() < 1.0, d
+    # the replicas of init() are back
+    mmff.download()
+    assert mmff.gpu_atoms.shape == (8, 38, 4) and np.isfinite(mmff.gpu_atoms).all()
     mmff.saveXYZ(str(tmp_path / "out.xyz"), "#test", 1)
     assert (tmp_path / "out.xyz").read_text().startswith("24\n")
     assert mmff.getTypeName(0) in ("C", "N", "O")

@@ -194,3 +194,28 @@ def test_trained_proposal_gain_over_plain_fire(world, golden):
           f"learned {np.median(sl['nsteps'][sl['status'] == 1])}; same minimum for "
           f"{int((dE <= 1e-5).sum())} of {int(both.sum())}")
     assert np.median(dE) <= 1e-5
+
+
+def test_rigid_projection_vs_oracle(world, golden):
+    """The rigid-body projection of warm-start moves (rigid_kernel) against its
+    FP64 restatement, and the move it makes keeps every bond length."""
+    grid = grid_from_golden(golden)
+    b = S.make_systems([24, 57, 130, 260], seed=8, topo_mode=1, sigma=0.1, cell=(22.56, 22.56, 40.0))
+    world.set_params(flags=DEFAULT_FLAGS)
+    world.grid_upload(golden["C"], grid)
+    world.upload(b)
+    prop = L.Proposal()
+    pos = L.atom_rows(b, world.state()["pos"])
+    rng = np.random.default_rng(1)
+    disp = rng.normal(0, 0.2, pos.shape) + np.array([0.3, -0.1, -0.5])
+    out = prop.project(disp)
+    ref = M.rigid_projection(pos, disp, b.natoms)
+    assert np.abs(out - ref).max() <= 2e-5 * np.abs(ref).max(), np.abs(out - ref).max()
+    # a rigid move: distances inside each molecule unchanged
+    moved = pos + ref
+    o = 0
+    for n in b.natoms:
+        d0 = np.linalg.norm(pos[o:o + n, None] - pos[None, o:o + n], axis=2)
+        d1 = np.linalg.norm(moved[o:o + n, None] - moved[None, o:o + n], axis=2)
+        assert np.abs(d1 - d0).max() < 1e-9
+        o += n

@@ -290,3 +290,47 @@ def test_surface_direct_term_vs_oracle(world, golden):
     assert np.allclose(E[:, 2], Es, rtol=1e-5, atol=1e-5), (E[:, 2], Es)
     world.lib.mmff_surf_upload(0, None, None, None, None, 1.0)
     world.set_params(flags=DEFAULT_FLAGS)
+
+
+def test_position_springs_vs_oracle(world, golden):
+    """Per-atom position springs (relax_multi.cl:995-1010): anchors 0.3 A away
+    from three atoms of every system, anisotropic constants; the relaxed
+    geometries and energies match the FP64 oracle with the same springs, and
+    eval reports the forces without them."""
+    grid = grid_from_golden(golden)
+    b = S.make_systems([24] * 8, seed=5, topo_mode=0, sigma=0.05, rotate=False, cell=(11.28, 11.28, 40.0))
+    world.set_params(flags=DEFAULT_FLAGS)
+    world.set_fire(FireParams(Flim=10.0))
+    world.upload(b)
+    pos0 = world.state()["pos"]
+    a, n, v = b.offsets()
+    anchor = np.zeros((int(b.natoms.sum()), 4)); anchor[:, 3] = -1.0
+    K = np.zeros((int(b.natoms.sum()), 3))
+    for s in range(b.nsys):
+        for k, ia in enumerate((0, 5, 17)):
+            anchor[a[s] + ia, :3] = pos0[v[s] + ia] + np.array([0.3, -0.2, 0.1]) * (1 + 0.1 * k)
+            anchor[a[s] + ia, 3] = 1.0
+            K[a[s] + ia] = (1.0, 2.0, 0.5)
+    world.set_constraints(anchor, K)
+    F0, _ = world.eval(False)
+    Fo0, _ = O.eval_forces(b, O.make_params(grid), golden["C"], pos=pos0)
+    assert np.abs(F0 - Fo0).max() <= 1e-5 * np.abs(Fo0).max()         # eval: no springs
+    world.relax(6000, 1e-4, conv_mode=1)
+    st = world.state()
+    Kc = np.zeros((K.shape[0], 4)); Kc[:, :3] = K
+    r = O.relax(b, O.make_params(grid), O.make_fire(Flim=10.0), golden["C"], niter=6000, Fconv=1e-4, conv_mode=1,
+                pos=pos0, constr=anchor, constrK=Kc)
+    world.set_constraints(None)
+    world.set_fire(FireParams())
+    assert (st["status"] == 1).all() and (r["converged"] == 1).all()
+    for s in range(b.nsys):
+        na = b.natoms[s]
+        d = st["pos"][v[s]:v[s] + na] - r["pos"][v[s]:v[s] + na]
+        assert np.sqrt((d ** 2).sum(1).mean()) <= 1e-2, s
+        # the springs hold: anchored atoms moved toward their anchors
+        for ia in (0, 5, 17):
+            assert np.linalg.norm(st["pos"][v[s] + ia] - anchor[a[s] + ia, :3]) < np.linalg.norm(
+                pos0[v[s] + ia] - anchor[a[s] + ia, :3]), (s, ia)
+    _, Eg = O.eval_forces(b, O.make_params(grid), golden["C"], pos=st["pos"])
+    _, Ec = O.eval_forces(b, O.make_params(grid), golden["C"], pos=r["pos"])
+    assert (np.abs(Eg[:, 3] - Ec[:, 3]) / b.natoms).max() <= 1e-5
