@@ -151,7 +151,7 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     from firecore_b200 import _lib
-    from firecore_b200.world import DEFAULT_FLAGS, FireParams, World
+    from firecore_b200.world import DEFAULT_FLAGS, NONBONDED, PBC, FireParams, World
     lib = _lib.load()
     sub, batch = workload(rank, args.nsys, args.workload)
     w = World(lrank)
@@ -159,7 +159,9 @@ def run_ours(args):
     C = w.grid_build(sub, return_coefs=True)
     w.sync()
     grid_build_s = time.perf_counter() - t0
-    w.set_params(flags=DEFAULT_FLAGS, npbc=(1, 1, 0), Rcut=RCUT)
+    # --terms pairs (profiling only): the relax kernels with the pair term alone
+    pairs_only = args.terms == "pairs"
+    w.set_params(flags=(NONBONDED | PBC) if pairs_only else DEFAULT_FLAGS, npbc=(1, 1, 0), Rcut=RCUT)
     w.set_fire(FireParams(Flim=FLIM))
     w.upload(batch)
     nsys = batch.nsys
@@ -181,7 +183,11 @@ def run_ours(args):
     pair_images, grid_samples, force_evals = int(cnt[0]), int(cnt[1]), int(cnt[2])
     lib.mmff_set_counting(0)
     st0 = w.state()
-    attr_t, attr_pairs, attr_grid = term_attribution(w, lib)
+    if pairs_only:
+        args.no_cpu = args.no_e2e = True
+        attr_t, attr_pairs, attr_grid = {"all": 1.0, "no_pairs": 1.0, "no_grid": 1.0}, 0, 0
+    else:
+        attr_t, attr_pairs, attr_grid = term_attribution(w, lib)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")   # > 126 MB L2
 
     def one_step():
@@ -245,7 +251,7 @@ def run_ours(args):
     pair_tf = PAIR_FLOPS * attr_pairs / t_pair / 1e12 if t_pair > 0 else None
     grid_term_gbs = GRID_BYTES * attr_grid / t_grid / 1e9 if t_grid > 0 else None
     out = None
-    parity = parity_subset(w, batch, sub, C) if rank == 0 else None
+    parity = parity_subset(w, batch, sub, C) if (rank == 0 and not pairs_only) else None
     if rank == 0:
         cpu = cpu_baseline(batch, sub, C, args, st0) if not args.no_cpu else None
         if cpu:
@@ -253,7 +259,8 @@ def run_ours(args):
         nconv0 = int((st0["status"] == 1).sum())
         steps_conv = st0["nsteps"][st0["status"] == 1]
         out = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": wsize, "steps": args.steps,
+            "metric": METRIC if not pairs_only else "profiling: relax kernels with the pair term only (not the metric)",
+            "value": value, "unit": UNIT, "n_gpus": wsize, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 forces / f64 FIRE reductions", "data": "synthetic (seeded generator)",
             "config": {"workload": workload_name(args),
@@ -450,6 +457,7 @@ LEARNED_METRIC = "relaxed systems/s to Fmax<1e-4 eV/A on 1 B200: learned+batched
 SNAPSHOTS = (0, 25, 100, 400)       # FIRE steps at which training descriptors are taken
 NWARM = 2                           # learned warm-start moves per system
 PROJECTION = 1                      # warm-start moves: rigid-body projection of the network's displacements
+TRAIN_TARGET = "rigid"              # training targets: the rigid-body part of the displacement to the minimum
 
 
 def learned_name(args):
@@ -512,7 +520,8 @@ def run_learned(args):
     t0 = time.perf_counter()
     train = S.config_uneven(seed=1001 + 7919 * rank, nsys=args.train_sys)
     w.upload(train)
-    F, T = L.trajectory_dataset(w, prop, train, snapshots=SNAPSHOTS, nstep_max=MAXSTEPS, Fconv=FCONV)
+    F, T = L.trajectory_dataset(w, prop, train, snapshots=SNAPSHOTS, nstep_max=MAXSTEPS, Fconv=FCONV,
+                                target=TRAIN_TARGET)
     data_s = time.perf_counter() - t0
     rng = np.random.default_rng(0)
     perm = rng.permutation(len(F))
@@ -664,7 +673,8 @@ def run_learned(args):
             "autotune": {"seconds": tune_s, "chosen": {str(k): v for k, v in w.tuning().items()},
                          "candidates": [[r["size_class"], r["kind"], r["threads"], r["pair_lanes"],
                                          round(r["us_per_system_step"], 4)] for r in tune_rows]},
-            "training": {"rows": int(len(F)), "snapshots": list(SNAPSHOTS), "steps": args.train_steps,
+            "training": {"rows": int(len(F)), "snapshots": list(SNAPSHOTS), "target": TRAIN_TARGET,
+                         "steps": args.train_steps,
                          "batch_atoms": 512 * 128, "first_loss": float(losses[0]),
                          "last_loss": float(np.mean(losses[-20:])), "train_ms": train_ms, "data_generation_s": data_s},
         }
@@ -858,6 +868,8 @@ def main():
     ap.add_argument("--train-steps", type=int, default=2000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--terms", default="all", choices=["all", "pairs"],
+                    help="replicas / uneven: 'pairs' runs the relax kernels with the pair term alone (profiling only)")
     ap.add_argument("--no-refsem", action="store_true",
                     help="--workload learned: skip the GPU run on the reference's semantics")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner (heuristic shapes)")

@@ -134,12 +134,33 @@ def atom_rows(batch, pos_vecs):
     return np.concatenate([pos_vecs[v[s]:v[s] + batch.natoms[s]] for s in range(batch.nsys)])
 
 
+def rigid_part(p0, p1, natoms):
+    """Per system, the rigid-body move (Kabsch: rotation about the centroid and
+    translation) that best maps positions p0 onto p1, as per-atom
+    displacements [sum natoms, 3]: the part of a relaxation a rigid
+    warm-start move can make."""
+    out = np.zeros_like(p0, dtype=np.float64)
+    o = 0
+    for n in natoms:
+        a = np.asarray(p0[o:o + n], np.float64); b = np.asarray(p1[o:o + n], np.float64)
+        ca, cb = a.mean(0), b.mean(0)
+        U, _, Vt = np.linalg.svd((a - ca).T @ (b - cb))
+        d = np.sign(np.linalg.det(Vt.T @ U.T))
+        R = Vt.T @ np.diag([1.0, 1.0, d]) @ U.T
+        out[o:o + n] = (a - ca) @ R.T + cb - a
+        o += n
+    return out
+
+
 def trajectory_dataset(world, prop: Proposal, batch, snapshots=(0, 25, 100), nstep_max=4000, Fconv=1e-4,
-                       z_top: float = 0.0):
+                       z_top: float = 0.0, target: str = "full"):
     """(features, targets) pairs from the plain batched relaxer: descriptors at
     the given FIRE step counts and, as targets, the displacement from there to
-    the relaxed geometry; only systems that converge contribute.
-    ``world`` holds ``batch`` (uploaded, FIRE parameters set)."""
+    the relaxed geometry (target="full"), or only its rigid-body part per
+    molecule (target="rigid": what a rigid warm-start move can use, without
+    the conformational changes no local descriptor predicts); only systems
+    that converge contribute.  ``world`` holds ``batch`` (uploaded, FIRE
+    parameters set)."""
     prop.set_elements(batch.elements)
     NA = int(batch.natoms.sum())
     feats, poss = [], []
@@ -155,5 +176,8 @@ def trajectory_dataset(world, prop: Proposal, batch, snapshots=(0, 25, 100), nst
     final = atom_rows(batch, st["pos"])
     conv_atom = np.repeat(st["status"] == 1, batch.natoms)
     F = np.concatenate([f[conv_atom] for f in feats])
-    T = np.concatenate([(final - p)[conv_atom] for p in poss])
+    if target == "rigid":
+        T = np.concatenate([rigid_part(p, final, batch.natoms)[conv_atom] for p in poss])
+    else:
+        T = np.concatenate([(final - p)[conv_atom] for p in poss])
     return F, T
