@@ -51,9 +51,9 @@ FLIM = 10.0
 PAIR_FLOPS = 32          # algorithmic FP32 flops per pair-image (both directions counted)
 GRID_BYTES = 1024        # 64 float4 gathers per atom B-spline sample
 # DRAM bytes (read + write) per system-step of the relax kernel the autotuner
-# picks for this workload, from an ncu capture of that kernel on 4096 systems x
-# 200 steps (80.6 + 7.0 MB); scaled by the system-steps of a launch
-DRAM_BYTES_PER_SYSTEM_STEP = 106.9
+# picks for the 4096-replica workload, from an ncu capture of that kernel on
+# 4096 systems x 200 steps (98.6 + 54.9 MB); scaled by the system-steps of a launch
+DRAM_BYTES_PER_SYSTEM_STEP = 187.4
 
 
 def env_rank():

@@ -82,7 +82,7 @@ def _declare(lib):
         "mmff_mlp_infer": [c_int, c_void, c_void], "mmff_mlp_set_data": [c_int, c_void, c_void],
         "mmff_mlp_train": [c_int, c_int, c_double, c_double, c_void], "mmff_mlp_set_elements": [c_void],
         "mmff_mlp_features": [c_double, c_void], "mmff_mlp_warmstart": [c_int, c_double, c_void],
-        "mmff_mlp_set_projection": [c_int], "mmff_mlp_project": [c_void, c_void],
+        "mmff_mlp_set_projection": [c_int], "mmff_mlp_project": [c_void, c_void], "mmff_mlp_wait_test": [],
         "mmff_mlp_plan": [c_void], "mmff_mlp_layout": [c_void],
         "mmff_set_graph": [c_int], "mmff_set_md": [c_double, c_double, c_double, ctypes.c_ulonglong],
         "mmff_md": [c_int], "mmff_surf_upload": [c_int, c_void, c_void, c_void, c_void, c_double], "mmff_autotune": [c_int, c_int, c_void, c_int],

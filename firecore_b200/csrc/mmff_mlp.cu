@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -49,8 +50,9 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
-// bounded wait on an mbarrier phase (2^31 SM clocks, about a second); false on timeout
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+// bounded wait on an mbarrier phase (limit in SM clocks: 2^31, about a second,
+// in normal launches); false on timeout
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit) {
     const long long t0 = clock64();
     while (true) {
         uint32_t ok;
@@ -62,7 +64,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
             : "r"(bar), "r"(parity)
             : "memory");
         if (ok) return true;
-        if (clock64() - t0 > (1ll << 31)) return false;
+        if (clock64() - t0 > limit) return false;
     }
 }
 
@@ -158,6 +160,8 @@ struct NetArgs {
     int* err;
     int ntile, nrows;
     float inv_batch, out_scale;
+    long long wait_limit;    // SM clocks per completion wait before the CTA gives up
+    int no_issue;            // wait test only: issue no product and no commit, so the first wait runs out
 };
 
 constexpr int NET_THREADS = 256;
@@ -204,8 +208,8 @@ __global__ void __launch_bounds__(NET_THREADS, 1) mlp_kernel(NetArgs A) {
 
     // commit the issued chain and wait for it with every thread; uniform failure
     auto complete = [&]() -> bool {
-        if (tid == 0) tc_commit(bar);
-        const bool ok = mbar_wait(bar, phase);
+        if (tid == 0 && !A.no_issue) tc_commit(bar);
+        const bool ok = mbar_wait(bar, phase, A.wait_limit);
         phase ^= 1u;
         const int bad = __syncthreads_or(!ok);
         tc_after();
@@ -229,7 +233,7 @@ __global__ void __launch_bounds__(NET_THREADS, 1) mlp_kernel(NetArgs A) {
             for (int i = tid; i < TILE * K0 * 2 / 16; i += NET_THREADS) dst[i] = src[i];
         }
         sync_for_mma();
-        if (tid == 0) issue(sb, tbase, OP_L1, false);
+        if (tid == 0 && !A.no_issue) issue(sb, tbase, OP_L1, false);
         if (!complete()) { failed = true; break; }
         for (int c = c0; c < c1; c += 16) {          // H1 = silu(Z1 + b1)
             tm_ld16(trow + TM_Z1 + c, v);
@@ -238,7 +242,7 @@ __global__ void __launch_bounds__(NET_THREADS, 1) mlp_kernel(NetArgs A) {
             st_row16(sm + SM_H1, r, c, HID, v);
         }
         sync_for_mma();
-        if (tid == 0) issue(sb, tbase, OP_L2, false);
+        if (tid == 0 && !A.no_issue) issue(sb, tbase, OP_L2, false);
         if (!complete()) { failed = true; break; }
         for (int c = c0; c < c1; c += 16) {          // H2 = silu(Z2 + b2), S2 = silu'(Z2 + b2)
             tm_ld16(trow + TM_WORK + c, v);
@@ -248,7 +252,7 @@ __global__ void __launch_bounds__(NET_THREADS, 1) mlp_kernel(NetArgs A) {
             if (TRAIN) st_row16(sm + SM_S2, r, c, HID, w);
         }
         sync_for_mma();
-        if (tid == 0) issue(sb, tbase, OP_L3, false);
+        if (tid == 0 && !A.no_issue) issue(sb, tbase, OP_L3, false);
         if (!complete()) { failed = true; break; }
         if (half == 0) {
             tm_ld16(trow + TM_WORK, v);
@@ -274,7 +278,7 @@ __global__ void __launch_bounds__(NET_THREADS, 1) mlp_kernel(NetArgs A) {
             st_row16(sm + SM_DY, r, 0, NOP, w);
         }
         sync_for_mma();
-        if (tid == 0) { issue(sb, tbase, OP_DW3, acc); issue(sb, tbase, OP_DH2, false); }
+        if (tid == 0 && !A.no_issue) { issue(sb, tbase, OP_DW3, acc); issue(sb, tbase, OP_DH2, false); }
         if (!complete()) { failed = true; break; }
         for (int c = c0; c < c1; c += 16) {          // dZ2 = dH2 * S2 (in place of S2)
             tm_ld16(trow + TM_WORK + c, v);
@@ -284,7 +288,7 @@ __global__ void __launch_bounds__(NET_THREADS, 1) mlp_kernel(NetArgs A) {
             st_row16(sm + SM_S2, r, c, HID, v);
         }
         sync_for_mma();
-        if (tid == 0) { issue(sb, tbase, OP_DW2, acc); issue(sb, tbase, OP_DB2, acc); issue(sb, tbase, OP_DH1, false); }
+        if (tid == 0 && !A.no_issue) { issue(sb, tbase, OP_DW2, acc); issue(sb, tbase, OP_DB2, acc); issue(sb, tbase, OP_DH1, false); }
         if (!complete()) { failed = true; break; }
         for (int c = c0; c < c1; c += 16) {          // dZ1 = dH1 * silu'(Z1 + b1), into the H2 buffer
             tm_ld16(trow + TM_WORK + c, v);
@@ -294,7 +298,7 @@ __global__ void __launch_bounds__(NET_THREADS, 1) mlp_kernel(NetArgs A) {
             st_row16(sm + SM_H2, r, c, HID, v);
         }
         sync_for_mma();
-        if (tid == 0) { issue(sb, tbase, OP_DW1, acc); issue(sb, tbase, OP_DB1, acc); }
+        if (tid == 0 && !A.no_issue) { issue(sb, tbase, OP_DW1, acc); issue(sb, tbase, OP_DB1, acc); }
         if (!complete()) { failed = true; break; }
         done++;
     }
@@ -711,6 +715,7 @@ int run_net(bool train, const uint8_t* X, const float4* T, int ntile, int nrows,
     a.X = reinterpret_cast<const uint4*>(X); a.T = T; a.Wp = reinterpret_cast<const uint4*>(N.Wp.p);
     a.prm = N.prm.p; a.gpart = N.gpart.p; a.lpart = N.lpart.p; a.out = out; a.err = N.err.p;
     a.ntile = ntile; a.nrows = nrows; a.inv_batch = inv_batch; a.out_scale = N.out_scale;
+    a.wait_limit = 1ll << 31; a.no_issue = 0;
     if (train) {
         mlp_kernel<true><<<grid, NET_THREADS, SM_ALLOC, st>>>(a);
         mmff_count_launches(1);
@@ -938,6 +943,36 @@ int mmff_mlp_features(double z_top, float* out) {
     MCK(cudaMemcpyAsync(out, N.feat.p, (size_t)V.NA * NFEAT * sizeof(float), cudaMemcpyDeviceToHost, V.stream));
     MCK(cudaStreamSynchronize(V.stream));
     return 0;
+}
+
+// The bounded completion waits of the tensor-core kernel, exercised: one
+// inference launch (one CTA, one tile of zeros) that issues no product and
+// no commit, so its first wait on the completion barrier can only run out
+// (limit 2^20 SM clocks, about half a millisecond).  Nothing asynchronous is
+// in flight when it does, so the CTA sets the error flag, frees its TMEM and
+// returns.  Returns 1 when the timeout came back as the error status (the
+// flag is cleared again), 0 if it did not.
+int mmff_mlp_wait_test(void) {
+    if (need_params()) return -1;
+    cudaStream_t st = world_stream();
+    if (!st) return -1;
+    if (set_attr() || N.Xs.ensure((size_t)TILE * K0 * 2) || N.outs.ensure(TILE) || N.err.ensure(1)) return -1;
+    MCK(cudaMemsetAsync(N.Xs.p, 0, (size_t)TILE * K0 * 2, st));
+    MCK(cudaMemsetAsync(N.err.p, 0, sizeof(int), st));
+    NetArgs a;
+    memset(&a, 0, sizeof a);
+    a.X = reinterpret_cast<const uint4*>(N.Xs.p); a.Wp = reinterpret_cast<const uint4*>(N.Wp.p); a.prm = N.prm.p;
+    a.out = N.outs.p; a.err = N.err.p; a.ntile = 1; a.nrows = 1; a.out_scale = N.out_scale;
+    a.wait_limit = 1ll << 20; a.no_issue = 1;
+    mlp_kernel<false><<<1, NET_THREADS, SM_ALLOC, st>>>(a);
+    mmff_count_launches(1);
+    MCK(cudaGetLastError());
+    int h = 0;
+    MCK(cudaMemcpyAsync(&h, N.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MCK(cudaStreamSynchronize(st));
+    MCK(cudaMemsetAsync(N.err.p, 0, sizeof(int), st));
+    MCK(cudaStreamSynchronize(st));
+    return h == 1 ? 1 : 0;
 }
 
 // How warm-start moves use the network's per-atom displacements: 0 as they

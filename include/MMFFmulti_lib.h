@@ -329,6 +329,12 @@ int mmff_mlp_features(double z_top, float* out);
  * the least-squares rigid-body move (translation + rotation, FP64 fit), which
  * leaves every bonded term of the molecule unchanged. */
 int mmff_mlp_set_projection(int mode);
+/* No counterpart in the reference.  Exercises the bounded completion waits of
+ * the tensor-core kernel: one launch that issues no product and no commit, so
+ * its first wait can only run out (about half a millisecond); the CTA then
+ * sets the error flag, frees its TMEM and returns.  1: the timeout came back
+ * as the error status (flag cleared again); 0: it did not; < 0: error. */
+int mmff_mlp_wait_test(void);
 /* No counterpart in the reference.  That rigid-body projection of host
  * displacements disp [sum natoms][3] at the systems' current positions ->
  * out [sum natoms][3] (the warm start's kernel, for checks). */

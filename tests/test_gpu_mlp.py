@@ -219,3 +219,18 @@ def test_rigid_projection_vs_oracle(world, golden):
         d1 = np.linalg.norm(moved[o:o + n, None] - moved[None, o:o + n], axis=2)
         assert np.abs(d1 - d0).max() < 1e-9
         o += n
+
+
+def test_tensor_core_wait_timeout_reports_and_recovers(world):
+    """A completion wait of the tcgen05 kernel that nothing completes (a
+    launch that issues no product and no commit) runs out after its short
+    limit: the kernel returns the error status, frees its TMEM, and the next
+    inference on the same context gives the same outputs as before."""
+    p, F, mean, std, T, X = setup_net(5, 300)
+    prop = L.Proposal()
+    prop.set_params(p, mean, std, 1.0)
+    before = prop.infer(F)
+    assert prop.lib.mmff_kernel_launches() >= 0
+    assert prop.lib.mmff_mlp_wait_test() == 1
+    after = prop.infer(F)
+    assert np.array_equal(before, after)
