@@ -617,6 +617,7 @@ struct SmemLayout {
     int pos, vel, fasm, fnb, fgrid, REQ, PLQ, ng, ngC, bk, apar, bL, bK, ksp, kpp, fng, red;
     int cwords, cpref, ccnt, clist;     // per-image candidate lists (cutoff + PBC only)
     int facc, total;                    // fixed-point force sums of the central image [3 * maxNA] int64
+    int stage;                          // image tiles: per warp the 32 j of the current tile (pos, REQ), or -1
 };
 
 // number of shifted (non-central) PBC images of the pair term
@@ -670,6 +671,11 @@ __host__ __device__ inline SmemLayout smem_layout_(int maxNA, int maxNN, int T, 
     L.ccnt = take(4 * nimg);                // candidates per image
     L.clist = take(2 * nimg * maxNA);       // candidate atom indices per image, ascending
     L.facc = take(8 * 3 * maxNA);
+    // image tiles (blocks >= kImageTileMinThreads with candidate lists): the
+    // positions and parameters of a tile's 32 candidates j, copied once per
+    // tile so that the 32 rotation steps read them directly instead of through
+    // the candidate list
+    L.stage = (nimg > 0 && T >= kImageTileMinThreads) ? take(2 * 16 * 32 * L.nwarps) : -1;
     L.total = o;
     return L;
 }

@@ -477,11 +477,19 @@ struct Engine {
         bool ok;
         float e = 0.f;
         const int jlast = nJ - 1;
+        // the tile's 32 candidates j into this warp's staging slots (one
+        // indirect load per lane instead of one per rotation step)
+        float4* stg = at<float4>(L.stage) + 64 * warp;
+        {
+            const int jj = Jl[min(j0 + lane, jlast)];
+            stg[lane] = spos[jj];
+            stg[32 + lane] = sREQ[jj];
+        }
+        __syncwarp();
 #pragma unroll kTileUnroll
         for (int s = 0; s < 32; s++) {
             const int jl = (lane + s) & 31;
-            const int j = Jl[min(j0 + jl, jlast)];
-            const float4 pj = spos[j], Rj = sREQ[j];
+            const float4 pj = stg[jl], Rj = stg[32 + jl];
             const bool excl = (xm >> jl) & 1u;
             const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
             const float F = pair_force<ENERGY, HB>(dx, dy, dz, Ri, Rj, excl, Rc2, kq, rc, CUT, ok, e);
@@ -494,6 +502,7 @@ struct Engine {
             rj.y = __shfl_sync(0xffffffffu, rj.y, nxt);
             rj.z = __shfl_sync(0xffffffffu, rj.z, nxt);
         }
+        __syncwarp();                                         // staging slots free for the next tile
         if (vi) fix_add(facc + 3 * i, fi);
         if (j0 + lane < nJ) fix_add(facc + 3 * (int)Jl[j0 + lane], rj);
     }
