@@ -9,8 +9,10 @@ package instead of FireCore's OpenCL library.
     E = mmff.eval()
 
 The reference module's interface (pyBall/MMFF_multi.py) is mirrored function
-by function; the topology comes from this package's own builder (see
-include/MMFFmulti_lib.h), so parameter values differ from FireCore's tables.
+by function.  ``init`` types the molecule as FireCore does: with FireCore's
+tables from ``common_resources/`` under the working directory (the files the
+reference reads), else with the four table names passed to ``init``; only when
+neither exists does the library fall back to its own parameter table.
 """
 from __future__ import annotations
 

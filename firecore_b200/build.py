@@ -28,7 +28,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fopenmp",
             "--expt-relaxed-constexpr", "-ccbin", HOST_CXX, "-I", os.path.join(ROOT, "include"),
             "-I", CSRC, "-Xptxas", "-warn-spills"]
-CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-fopenmp", "-I", os.path.join(ROOT, "include"), "-I", CSRC]
+CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-fopenmp", "-ffp-contract=off", "-I", os.path.join(ROOT, "include"), "-I", CSRC]
 
 
 def _needs(obj, srcs):

@@ -8,12 +8,16 @@
 // same names and shapes (pyBall/MMFF_multi.py:210-257); the physics runs on the
 // GPU through mmff_systems_upload / mmff_relax / mmff_eval.
 //
-// Topology: the reference builds it with MM::Builder from AtomTypes.dat etc.;
-// here a small builder of this project (bond detection by covalent radii,
-// nodes = atoms with valence > 1, hybridisation from the bond count,
-// parameters from firecore_b200/csrc/mmff_params.h) fills the same
-// MMFFsp3_loc arrays.  Parameter values therefore differ from FireCore's
-// files; array meaning and layout do not.
+// Topology: as in the reference (MolWorld_sp3::init -> initParams /
+// buildMolecule_xyz / makeFFs), FireCore's parameter tables are read from
+// common_resources/{Element,Atom,Bond,Angle}Types.dat under the working
+// directory -- the reference reads exactly these and ignores init's four file
+// arguments (MMFFmulti_lib.cpp:85 has params.init commented out); if they are
+// absent, the caller's four names are tried.  mmff_builder.cpp then reproduces
+// MM::Builder's typing and toMMFFsp3_loc bit for bit.  Only when no tables are
+// found does a small builder of this project (bond detection by covalent
+// radii, nodes = atoms with valence > 1, parameters from mmff_params.h) fill
+// the same MMFFsp3_loc arrays with its own values.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -26,6 +30,7 @@
 #include <vector>
 
 #include "MMFFmulti_lib.h"
+#include "mmff_builder.h"
 #include "mmff_host.h"
 #include "mmff_params.h"
 
@@ -86,7 +91,9 @@ bool read_xyz(const char* fname, XYZ& X) {
 // one molecule in MMFFsp3_loc layout (nodes first)
 struct Molecule {
     int natoms = 0, nnode = 0;
-    std::vector<int> el;          // element index
+    std::vector<int> el;          // element index (built-in table)
+    std::vector<std::string> names;   // atom-type names (FireCore tables); empty with the built-in table
+    std::vector<int> neighCell;   // [natoms*4] image index per neighbour (cell read from the xyz); empty otherwise
     std::vector<V3> pos;          // [natoms + nnode]
     std::vector<int> neighs;      // [natoms*4]
     std::vector<int> bkneighs;    // [natoms*4]
@@ -176,6 +183,45 @@ bool build_from_xyz(const XYZ& X, Molecule& M, std::string& err) {
     return true;
 }
 
+// FireCore-typed molecule (mmff_builder.cpp) -> Molecule, with back neighbours
+bool from_built(const fcb::Built& B, const fcb::Tables& T, Molecule& M, std::string& err) {
+    M = Molecule();
+    M.natoms = B.natoms; M.nnode = B.nnode;
+    M.el.assign(B.natoms, EL_C);
+    for (int i = 0; i < B.natoms; i++) M.names.push_back(T.types[B.type[i]].name);
+    for (int i = 0; i < B.natoms + B.nnode; i++) M.pos.push_back(V3{B.pos[3 * i], B.pos[3 * i + 1], B.pos[3 * i + 2]});
+    M.neighs = B.neighs; M.REQ = B.REQ;
+    M.apars = B.apars; M.bLs = B.bLs; M.bKs = B.bKs; M.Ksp = B.Ksp; M.Kpp = B.Kpp;
+    if (B.pbc) M.neighCell = B.neighCell;
+    M.bkneighs.assign(4 * (size_t)B.natoms, -1);
+    for (int ia = 0; ia < B.nnode; ia++) for (int j = 0; j < 4; j++) {   // MMFFsp3_loc::makeBackNeighs
+        const int ja = M.neighs[4 * ia + j];
+        if (ja < 0) continue;
+        int q = 0;
+        while (q < 4 && M.bkneighs[4 * ja + q] >= 0) q++;
+        if (q == 4) { err = "atom with more than 4 back-neighbours"; return false; }
+        M.bkneighs[4 * ja + q] = ia * 4 + j;
+    }
+    return true;
+}
+
+bool file_exists(const char* f) { if (!f) return false; FILE* fp = fopen(f, "r"); if (fp) fclose(fp); return fp != nullptr; }
+
+// FireCore's tables: common_resources/ under the working directory (what the
+// reference reads), else the four names init was given; false if neither set exists
+bool find_tables(const char* e, const char* a, const char* b, const char* g, fcb::Tables& T, std::string& err) {
+    const char* cr[4] = {"common_resources/ElementTypes.dat", "common_resources/AtomTypes.dat", "common_resources/BondTypes.dat",
+                         "common_resources/AngleTypes.dat"};
+    const char* given[4] = {e, a, b, g};
+    for (const char** set : {cr, given}) {
+        if (!(file_exists(set[0]) && file_exists(set[1]) && file_exists(set[2]) && file_exists(set[3]))) continue;
+        if (fcb::load_tables(set[0], set[1], set[2], set[3], T, err)) return true;
+        return false;
+    }
+    err.clear();
+    return false;
+}
+
 // ---------------------------------------------------------------- the world
 struct LegacyWorld {
     bool ready = false;
@@ -185,6 +231,8 @@ struct LegacyWorld {
     int nPBC[3] = {1, 1, 0};
     int flags = 1 | 2 | 4 | 8 | 16 | 128 | 256 | 512;
     bool bGrid = false;
+    bool fc_tables = false;       // FireCore's tables were found and typed the molecule
+    fcb::Tables tables;
     // FIRE (set_opt) -- pyBall/MMFF_multi.py:349 defaults
     double fire[9] = {0.1, 0.02, 0.2, 1.1, 0.5, 0.8, 5, 0.0, 10.0};
     // thermal drive of init(T, gamma) (MolWorld_sp3_multi's TDrive): MDloop runs
@@ -366,17 +414,27 @@ void setVerbosity(int verbosity_, int idebug_) { g_verbosity = verbosity_; (void
 void* init(int nSys, char* xyz_name, char* surf_name, char* smile_name, bool bMMFF, bool bEpairs, int* nPBC, int* grid_nPBC,
            double gridStep, char* sElementTypes, char* sAtomTypes, char* sBondTypes, char* sAngleTypes, double T, double gamma,
            int nExplore, int nRelax, double pos_kick, double vel_kick, int GridFF) {
-    (void)smile_name; (void)bMMFF; (void)bEpairs; (void)sElementTypes; (void)sAtomTypes; (void)sBondTypes; (void)sAngleTypes;
-    (void)nExplore; (void)nRelax; (void)pos_kick; (void)vel_kick;
+    (void)smile_name; (void)bMMFF; (void)nExplore; (void)nRelax; (void)pos_kick; (void)vel_kick;
     L.T = T; L.gamma = gamma; L.md_set = false;
     if (nSys < 1 || !xyz_name) { set_error("init: need nSys >= 1 and an xyz file"); return nullptr; }
     if (mmff_init_device(0)) { set_error(std::string("init: ") + mmff_last_error()); return nullptr; }
     XYZ X;
     std::string fn = xyz_name;
-    if (!read_xyz(fn.c_str(), X) && !read_xyz((fn + ".xyz").c_str(), X)) { set_error("init: cannot read " + fn); return nullptr; }
+    // MolWorld_sp3::insertMolecule appends ".xyz" to a name without extension
+    if (!read_xyz(fn.c_str(), X)) {
+        fn += ".xyz";
+        if (!read_xyz(fn.c_str(), X)) { set_error("init: cannot read " + std::string(xyz_name)); return nullptr; }
+    }
     std::string err;
-    if (!build_from_xyz(X, L.mol, err)) { set_error("init: " + err); return nullptr; }
     if (nPBC) for (int k = 0; k < 3; k++) L.nPBC[k] = nPBC[k];
+    L.fc_tables = find_tables(sElementTypes, sAtomTypes, sBondTypes, sAngleTypes, L.tables, err);
+    if (!L.fc_tables && !err.empty()) { set_error("init: " + err); return nullptr; }
+    if (L.fc_tables) {
+        fcb::Built B;
+        if (!fcb::build_xyz(L.tables, fn.c_str(), bEpairs, L.nPBC, B, err) || !from_built(B, L.tables, L.mol, err)) {
+            set_error("init: " + err); return nullptr;
+        }
+    } else if (!build_from_xyz(X, L.mol, err)) { set_error("init: " + err); return nullptr; }
     L.nSys = nSys;
     const int na = L.mol.natoms, nn = L.mol.nnode, nv = na + nn;
     if (X.has_lvs) memcpy(L.lvec, X.lvs, sizeof L.lvec);
@@ -391,10 +449,14 @@ void* init(int nSys, char* xyz_name, char* surf_name, char* smile_name, bool bMM
         std::vector<double> spos(3 * nsub), sREQ(4 * nsub);
         double ztop = -1e300;
         for (int i = 0; i < nsub; i++) {
-            const int e = elem_index(S.el[i].c_str());
-            const Elem& E = kElem[e < 0 ? EL_C : e];
             spos[3 * i] = S.pos[i].x; spos[3 * i + 1] = S.pos[i].y; spos[3 * i + 2] = S.pos[i].z;
-            sREQ[4 * i] = E.R0; sREQ[4 * i + 1] = std::sqrt(E.E0); sREQ[4 * i + 2] = S.q[i]; sREQ[4 * i + 3] = 0;
+            if (L.fc_tables) {   // MolWorld_sp3::loadSurf reads the substrate through MMFFparams::loadXYZ
+                fcb::substrate_REQ(L.tables, S.el[i], S.q[i], 0.0, &sREQ[4 * i]);
+            } else {
+                const int e = elem_index(S.el[i].c_str());
+                const Elem& E = kElem[e < 0 ? EL_C : e];
+                sREQ[4 * i] = E.R0; sREQ[4 * i + 1] = std::sqrt(E.E0); sREQ[4 * i + 2] = S.q[i]; sREQ[4 * i + 3] = 0;
+            }
             ztop = std::max(ztop, S.pos[i].z);
         }
         const double step = gridStep > 0 ? gridStep : 0.1;
@@ -429,7 +491,7 @@ void* init(int nSys, char* xyz_name, char* surf_name, char* smile_name, bool bMM
         for (int a = 0; a < na; a++) for (int k = 0; k < 4; k++) {
             const int j = L.mol.neighs[4 * a + k];
             L.gneighs[4 * ((size_t)s * nv + a) + k] = j;
-            L.gneighCell[4 * ((size_t)s * nv + a) + k] = j >= 0 ? central : -1;
+            L.gneighCell[4 * ((size_t)s * nv + a) + k] = j < 0 ? -1 : (L.mol.neighCell.empty() ? central : L.mol.neighCell[4 * a + k]);
             L.gbkNeighs[4 * ((size_t)s * nv + a) + k] = L.mol.bkneighs[4 * a + k];
             L.REQs[4 * ((size_t)s * na + a) + k] = (float)L.mol.REQ[4 * a + k];
         }
@@ -696,7 +758,7 @@ int saveXYZ(const char* fname, const char* comment, int imod) {
     const int s = (imod > 0 && imod <= L.nSys) ? imod - 1 : L.iSystemCur;
     fprintf(f, "%i\n%s\n", na, comment ? comment : "");
     for (int i = 0; i < na; i++)
-        fprintf(f, "%s %12.6f %12.6f %12.6f\n", kElem[L.mol.el[i]].sym, L.atoms[4 * ((size_t)s * nv + i)],
+        fprintf(f, "%s %12.6f %12.6f %12.6f\n", L.mol.names.empty() ? kElem[L.mol.el[i]].sym : L.mol.names[i].c_str(), L.atoms[4 * ((size_t)s * nv + i)],
                 L.atoms[4 * ((size_t)s * nv + i) + 1], L.atoms[4 * ((size_t)s * nv + i) + 2]);
     fclose(f);
     return na;
@@ -705,7 +767,7 @@ int saveXYZ(const char* fname, const char* comment, int imod) {
 const char* getTypeName(int ia, bool fromFF) {
     (void)fromFF;
     if (!L.ready || ia < 0 || ia >= L.mol.natoms) return "?";
-    return kElem[L.mol.el[ia]].sym;
+    return L.mol.names.empty() ? kElem[L.mol.el[ia]].sym : L.mol.names[ia].c_str();
 }
 
 double eval() {

@@ -214,6 +214,27 @@ int mmff_gen_systems(int nsys, const int* natoms, uint64_t seed, int topo_mode, 
 int mmff_gen_slab(double a, int ncell, int layers, double z_top, double q, const double* REQ_cation,
                   const double* REQ_anion, double* spos, double* sREQ);
 
+/* ------------------------------------------------------------ FireCore topology builder (host only)
+ * Replaces what MolWorld_sp3::init does before any force evaluation
+ * (cpp/common/molecular/MolWorld_sp3.h:309-382): initParams (:1298) reads the
+ * four tables with MMFFparams (MMFFparams.h:267-541), buildMolecule_xyz
+ * (:1323) and makeFFs / makeMMFFs (:1359-1586) type the molecule with
+ * MM::Builder (autoBonds, autoConfEPi, assignBondParams, assignTypes,
+ * toMMFFsp3_loc: MMFFBuilder.h:2087, 1633, 867, 1444, 4153) and fill
+ * MMFFsp3_loc.  Same outputs, bit for bit, on the same files.
+ * Arrays are the caller's, sized for cap atoms: apos [2*cap*3] (natoms atoms,
+ * then nnode pi orientations), REQs / neighs / neighCell [cap*4], atypes
+ * [cap], apars / bLs / bKs / Ksp / Kpp [cap*4] (nnode rows), type_names
+ * [cap*8] (NUL-padded); any may be NULL.  counts[4] = natoms, nnode,
+ * natoms + nnode, 1 if the xyz carried an "lvs" cell (then neighCell holds the
+ * image of each bonded neighbour for the nPBC images, else -1).  bEpairs as in
+ * FireCore's init.  Returns natoms; -1 on bad files or a molecule FireCore's
+ * builder rejects (message in mmff_last_error), -2 if cap is too small. */
+int mmff_build_xyz(const char* fElementTypes, const char* fAtomTypes, const char* fBondTypes, const char* fAngleTypes,
+                   const char* xyz, int bEpairs, const int* nPBC, int cap, int* counts, double* apos, double* REQs,
+                   int* atypes, int* neighs, int* neighCell, double* apars, double* bLs, double* bKs, double* Ksp,
+                   double* Kpp, char* type_names);
+
 
 /* ============================================================================
  * Legacy symbols: the reference library's ABI as pyBall/MMFF_multi.py binds it
@@ -235,6 +256,13 @@ void* init(int nSys, char* xyz_name, char* surf_name, char* smile_name, bool bMM
            int* grid_nPBC, double gridStep, char* sElementTypes, char* sAtomTypes, char* sBondTypes,
            char* sAngleTypes, double T, double gamma, int nExplore, int nRelax, double pos_kick, double vel_kick,
            int GridFF);                                                     /* :75 */
+/* init: as MolWorld_sp3::init does, the molecule is typed with FireCore's tables
+ * from common_resources/{Element,Atom,Bond,Angle}Types.dat under the working
+ * directory (the reference ignores the four file arguments, MMFFmulti_lib.cpp:85);
+ * when those are absent the four names given are used, and when neither set
+ * exists this library's own parameter table (a documented deviation).  Typing
+ * with tables = mmff_build_xyz.  smile_name, nExplore, nRelax, pos_kick and
+ * vel_kick are not used. */
 int   run(int nstepMax, double dt, double Fconv, int ialg, double* outE, double* outF, int iParalel);   /* :116 */
 void  MDloop(int perframe, double Ftol, int iParalel, int perVF);           /* :134 */
 void  set_opt(double dt_max, double dt_min, double damp_max, double finc, double fdec, double falpha, int minLastNeg,

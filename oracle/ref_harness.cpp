@@ -196,4 +196,46 @@ void ref_grid_points(int npt, const double* pts, int nsub, const double* spos, c
     delete[] sm; delete[] sc;
 }
 
+// FireCore's own topology / parameter builder on one xyz file, the path the
+// drop-in init takes (MolWorld_sp3::init, MolWorld_sp3.h:309-382):
+// initParams (:1298-1315) -> buildMolecule_xyz (:1323-1351) -> makeFFs
+// (:1442-1586, makeMMFFs -> MM::Builder::assignTypes / toMMFFsp3_loc,
+// MMFFBuilder.h:1444, 4153).  A fresh MolWorld_sp3 per call.  Outputs (caller
+// capacity cap atoms; returns natoms, or -1 when cap is too small):
+//   counts[4] = natoms, nnode, nvecs, bPBC
+//   apos [cap*2*3] (nvecs rows), REQs [cap*4], atypes [cap], neighs / neighCell [cap*4],
+//   apars / bLs / bKs / Ksp / Kpp [cap*4] (nnode rows), type_names [cap*8] chars
+int ref_build_xyz(const char* fElem, const char* fAtom, const char* fBond, const char* fAngle, const char* fDih,
+                  const char* xyz, int bEpairs, const int* nPBC, int cap, int* counts, double* apos, double* REQs,
+                  int* atypes, int* neighs, int* neighCell, double* apars, double* bLs, double* bKs, double* Ksp,
+                  double* Kpp, char* type_names) {
+    verbosity = 0;
+    MolWorld_sp3* w = new MolWorld_sp3();
+    w->bEpairs = bEpairs != 0;
+    w->nPBC = Vec3i{nPBC[0], nPBC[1], nPBC[2]};
+    w->bOptimizer = false;
+    w->initParams(fElem, fAtom, fBond, fAngle, fDih);
+    if (w->buildMolecule_xyz(xyz) < 0) return -2;
+    w->makeFFs();
+    MMFFsp3_loc& f = w->ffl;
+    if (f.natoms > cap) return -1;
+    counts[0] = f.natoms; counts[1] = f.nnode; counts[2] = f.nvecs; counts[3] = w->bPBC ? 1 : 0;
+    for (int i = 0; i < f.nvecs; i++) { apos[3 * i] = f.apos[i].x; apos[3 * i + 1] = f.apos[i].y; apos[3 * i + 2] = f.apos[i].z; }
+    for (int i = 0; i < f.natoms; i++) {
+        for (int k = 0; k < 4; k++) {
+            REQs[4 * i + k] = f.REQs[i].array[k];
+            neighs[4 * i + k] = f.neighs[i].array[k];
+            neighCell[4 * i + k] = w->bPBC ? f.neighCell[i].array[k] : -1;
+        }
+        atypes[i] = f.atypes[i];
+        const char* nm = (f.atypes[i] >= 0) ? w->params.atypes[f.atypes[i]].name : "?";
+        strncpy(type_names + 8 * i, nm, 8);
+    }
+    for (int i = 0; i < f.nnode; i++) for (int k = 0; k < 4; k++) {
+        apars[4 * i + k] = f.apars[i].array[k]; bLs[4 * i + k] = f.bLs[i].array[k]; bKs[4 * i + k] = f.bKs[i].array[k];
+        Ksp[4 * i + k] = f.Ksp[i].array[k]; Kpp[4 * i + k] = f.Kpp[i].array[k];
+    }
+    return f.natoms;
+}
+
 }  // extern "C"

@@ -47,3 +47,42 @@ def test_legacy_init_run_eval_scan(tmp_path):
     mmff.saveXYZ(str(tmp_path / "out.xyz"), "#test", 1)
     assert (tmp_path / "out.xyz").read_text().startswith("24\n")
     assert mmff.getTypeName(0) in ("C", "N", "O")
+
+
+def test_legacy_init_types_with_firecore_tables(tmp_path, monkeypatch):
+    """init reads FireCore-format tables from common_resources/ under the working
+    directory (as MolWorld_sp3::init does), types the molecule with
+    mmff_build_xyz, and the device world evaluates that force field: forces and
+    energy against the FP64 oracle on the same arrays."""
+    from builder_tables import write_tables
+    from firecore_b200 import MMFF_multi as mmff
+    from firecore_b200 import topology as T
+    from oracle import oracle as O
+    O.build_oracle()
+    tables = write_tables(str(tmp_path / "common_resources"))
+    monkeypatch.chdir(tmp_path)
+    xyz = os.path.join(HERE, "mol24.xyz")
+    mmff.init(nSys_=4, xyz_name=xyz, nPBC=(1, 1, 0))
+    mmff.getBuffs()
+    d = T.build_xyz(xyz, tables)
+    na, nn = d["natoms"], d["nnode"]
+    assert mmff.natoms == na and mmff.nnode == nn
+    assert [mmff.getTypeName(i) for i in range(na)] == d["type_names"]
+    for buf, key in ((mmff.gpu_REQs, "REQs"), (mmff.gpu_MMpars, "apars"), (mmff.gpu_BLs, "bLs"), (mmff.gpu_BKs, "bKs"),
+                     (mmff.gpu_Ksp, "Ksp"), (mmff.gpu_Kpp, "Kpp")):
+        np.testing.assert_array_equal(buf[3], d[key].astype(np.float32), err_msg=key)
+    np.testing.assert_array_equal(mmff.gpu_atoms[0, :, :3], d["apos"].astype(np.float32))
+    np.testing.assert_array_equal(mmff.gpu_neighs[0, :na], d["neighs"])
+    E = mmff.eval()
+    b = T.to_batch(d)
+    b.pos = mmff.gpu_atoms[0, :, :3].astype(np.float64)          # the float32 positions the device holds
+    Fo, Eo = O.eval_forces(b, O.make_params(flags=O.DEFAULT_FLAGS, npbc=(1, 1, 0)))
+    assert abs(E - Eo[0, 3]) <= 2e-6 * max(1.0, abs(Eo[0, 3])), (E, Eo[0])
+    F = mmff.gpu_aforces[0, :, :3]
+    scale = np.abs(Fo).max()
+    assert np.abs(F - Fo).max() <= 2e-5 * scale, (np.abs(F - Fo).max(), scale)
+    # and it relaxes
+    mmff.set_opt(dt_max=0.05, dt_min=0.005, damp_max=0.1, minLastNeg=3)
+    n = mmff.run(nstepMax=2000, Fconv=1e-3)
+    assert 0 < n <= 2000 and np.isfinite(mmff.gpu_atoms).all()
+    assert mmff.eval() < E
