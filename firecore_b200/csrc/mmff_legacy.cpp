@@ -416,6 +416,10 @@ void* init(int nSys, char* xyz_name, char* surf_name, char* smile_name, bool bMM
            int nExplore, int nRelax, double pos_kick, double vel_kick, int GridFF) {
     (void)smile_name; (void)bMMFF; (void)nExplore; (void)nRelax; (void)pos_kick; (void)vel_kick;
     L.T = T; L.gamma = gamma; L.md_set = false;
+    {   // a new world: the cell of an earlier init (its substrate or xyz) does not carry over
+        const double lv0[9] = {20, 0, 0, 0, 20, 0, 0, 0, 20};
+        memcpy(L.lvec, lv0, sizeof L.lvec);
+    }
     if (nSys < 1 || !xyz_name) { set_error("init: need nSys >= 1 and an xyz file"); return nullptr; }
     if (mmff_init_device(0)) { set_error(std::string("init: ") + mmff_last_error()); return nullptr; }
     XYZ X;
