@@ -95,6 +95,27 @@ _sig("scanRotation", [c_int, c_int_p, c_int, c_int, c_int, c_double, c_int, c_do
 _sig("scan", [c_int] + [c_double_p] * 5 + [c_bool, c_bool, c_int, c_double, c_double, c_double])
 
 isInitialized = False
+
+
+def addDistConstrain(i0, i1, lmin=1, lmax=1, kmin=1, kmax=1, flim=1e+300, l=None, k=None, shift=(0., 0., 0.),
+                     bOldIndex=False):
+    """Flat-bottom spring between atoms i0 and i1 of every replica (l / k set
+    both bounds / both constants), applied by the next relaxations.
+    bOldIndex: indices count atoms in the input order."""
+    if l is not None:
+        lmin = lmax = l
+    if k is not None:
+        kmin = kmax = k
+    sh = np.ascontiguousarray(shift, np.float64)
+    return lib.addDistConstrain(i0, i1, lmin, lmax, kmin, kmax, flim, _np_as(sh, c_double_p), bOldIndex)
+
+
+def addAngConstrain(i0, i1, i2, ang0=0.0, k=1.0):
+    """Hold the angle i1-i0-i2 (i0 the centre) at ang0 [rad]; active once a
+    distance constraint exists, as in FireCore."""
+    return lib.addAngConstrain(i0, i1, i2, ang0, k)
+
+
 glob_bMMFF = True
 nSys = 0
 

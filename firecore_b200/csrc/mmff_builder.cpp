@@ -432,6 +432,7 @@ bool build_xyz(const Tables& T, const char* xyz, bool epairs, const int nPBC[3],
             if (old[i].conf >= 0) W.confs[old[i].conf].atom = perm[i];
         }
         for (Bond& b : W.bonds) { b.a = perm[b.a]; b.b = perm[b.b]; if (b.a > b.b) std::swap(b.a, b.b); }
+        M.permut = perm;                       // Builder::setup_atom_permut
     }
     // ---- atom types: hybridisation sub-types, then the special-type rules
     {

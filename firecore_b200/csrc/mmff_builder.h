@@ -53,6 +53,7 @@ struct Built {
     std::vector<int> type;            // natoms
     std::vector<int> neighs, neighCell;   // natoms x 4 (cells only with pbc)
     std::vector<double> apars, bLs, bKs, Ksp, Kpp;   // nnode x 4
+    std::vector<int> permut;          // builder order (xyz atoms read, then electron-pair caps) -> index here
 };
 
 // xyz -> Built.  epairs: FireCore's bEpairs (explicit electron pairs and the

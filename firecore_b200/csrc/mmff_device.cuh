@@ -32,6 +32,7 @@ enum : int {
     F_EXCL13 = 1 << 11,
     // set by the host for relaxations when position constraints are uploaded
     F_CONSTR = 1 << 12,
+    F_BCONS = 1 << 13,   // distance / angle constraints between atoms (Constrains bonds / angles)
 };
 
 // The host turns F_EXCL13 on exactly when the angle terms subtract the 1-3
@@ -113,6 +114,14 @@ struct Systems {
     const int* __restrict__ moff;       // per system: first word of its exclusion rows
     const float4* __restrict__ constr;  // per atom: spring anchor (local frame) and w > 0 = on (F_CONSTR)
     const float4* __restrict__ constrK; // per atom: spring constants (kx, ky, kz)
+    // distance / angle constraints (F_BCONS): (system, or -1 for every system; local atom indices)
+    const int4* __restrict__ dcon_i;    // (system, i0, i1, -)
+    const float4* __restrict__ dcon_a;  // (lmax, lmin, kmax, kmin)
+    const float4* __restrict__ dcon_b;  // (shift along a, b, c in cell units, flim)
+    int ndcon;
+    const int4* __restrict__ acon_i;    // (system, centre, end 1, end 2)
+    const float4* __restrict__ acon_a;  // (cos a0/2, sin a0/2, k, -)
+    int nacon;
     unsigned int* gkey;                 // per atom: stencil cell of its GridFF cache (0xffffffff: empty); null: no cache
     float4* gcs;                        // per atom: 16 float4 = PLQ . C of its 4x4x4 stencil ([x][y] rows of 4 z)
     float4* pos;                        // local frame
@@ -290,6 +299,55 @@ __device__ __forceinline__ float3 constraint_force(const Systems& Y, int ia, flo
         f.x = fmaf(c.x - p.x, fmaxf(k.x, 0.f), f.x);
         f.y = fmaf(c.y - p.y, fmaxf(k.y, 0.f), f.y);
         f.z = fmaf(c.z - p.z, fmaxf(k.z, 0.f), f.z);
+    }
+    return f;
+}
+
+// Distance and angle constraints acting on atom ia of system isys
+// (constrains.h: DistConstr::apply with Forces.h:161 spring, AngleConstr::apply
+// with evalAngleCosHalf; applied by MolWorld_sp3::run_no_omp after the force
+// field, MolWorld_sp3.h:2391-2395, so before the force clamp).  sp: the system's
+// positions, lv: its cell (rows a, b, c).  Each constraint is evaluated by each
+// of its atoms for its own share.
+static __device__ __forceinline__ float3 bond_constraint_force(const Systems& Y, int isys, int ia, const float4* sp, const float* lv,
+                                                     float3 f) {
+    for (int c = 0; c < Y.ndcon; c++) {
+        const int4 d = __ldg(Y.dcon_i + c);
+        if ((d.x >= 0 && d.x != isys) || (d.y != ia && d.z != ia)) continue;
+        const float4 A = __ldg(Y.dcon_a + c), B = __ldg(Y.dcon_b + c);
+        const float3 p0 = f3(sp[d.y]), p1 = f3(sp[d.z]);
+        const float3 dd = make_float3(p1.x - p0.x + (lv[0] * B.x + lv[3] * B.y + lv[6] * B.z),
+                                      p1.y - p0.y + (lv[1] * B.x + lv[4] * B.y + lv[7] * B.z),
+                                      p1.z - p0.z + (lv[2] * B.x + lv[5] * B.y + lv[8] * B.z));
+        const float l = sqrtf(dot3(dd, dd));
+        float fs = 0.f;                                   // flat-bottom spring between lmin and lmax
+        if (l > A.x) fs = fminf((l - A.x) * A.z, B.w);
+        else if (l < A.y) fs = fmaxf((l - A.y) * A.w, -B.w);
+        const float3 g = dd * (fs / l);
+        if (ia == d.y) f = f + g;
+        if (ia == d.z) f = f - g;
+    }
+    for (int c = 0; c < Y.nacon; c++) {
+        const int4 a = __ldg(Y.acon_i + c);
+        if ((a.x >= 0 && a.x != isys) || (a.y != ia && a.z != ia && a.w != ia)) continue;
+        const float4 A = __ldg(Y.acon_a + c);
+        const float3 pc = f3(sp[a.y]);
+        float3 h1 = pc - f3(sp[a.z]), h2 = pc - f3(sp[a.w]);
+        const float ir1 = rsqrtf(dot3(h1, h1)), ir2 = rsqrtf(dot3(h2, h2));
+        h1 = h1 * ir1; h2 = h2 * ir2;
+        const float3 h = h1 + h2;                          // evalAngleCosHalf (Forces.h:190)
+        float c2 = dot3(h, h) * 0.25f;
+        const float s2 = 1.f - c2 + 1e-14f;
+        const float cc = sqrtf(c2), ss = sqrtf(fmaxf(s2, 0.f));
+        const float csy = fmaf(A.y, cc, -A.x * ss);
+        float fr = -A.z * csy;
+        c2 *= -2.f;
+        fr = fr / (4.f * cc * ss);
+        const float fr1 = fr * ir1, fr2 = fr * ir2;
+        const float3 f1 = h * fr1 + h1 * (fr1 * c2), f2 = h * fr2 + h2 * (fr2 * c2);
+        if (ia == a.y) f = f + f1 + f2;
+        if (ia == a.z) f = f - f1;
+        if (ia == a.w) f = f - f2;
     }
     return f;
 }

@@ -94,6 +94,7 @@ struct Molecule {
     std::vector<int> el;          // element index (built-in table)
     std::vector<std::string> names;   // atom-type names (FireCore tables); empty with the built-in table
     std::vector<int> neighCell;   // [natoms*4] image index per neighbour (cell read from the xyz); empty otherwise
+    std::vector<int> permut;      // input (builder) order -> index here, MM::Builder::atom_permut
     std::vector<V3> pos;          // [natoms + nnode]
     std::vector<int> neighs;      // [natoms*4]
     std::vector<int> bkneighs;    // [natoms*4]
@@ -126,6 +127,7 @@ bool build_from_xyz(const XYZ& X, Molecule& M, std::string& err) {
     std::vector<int> inv(n);
     for (int k = 0; k < n; k++) inv[order[k]] = k;
     M.natoms = n; M.nnode = nnode;
+    M.permut = inv;
     M.el.resize(n); M.pos.assign(n + nnode, V3{0, 0, 0});
     M.neighs.assign(4 * n, -1); M.bkneighs.assign(4 * n, -1); M.REQ.assign(4 * n, 0.0);
     M.apars.assign(4 * nnode, 0.0); M.bLs.assign(4 * nnode, 0.0); M.bKs.assign(4 * nnode, 0.0);
@@ -193,6 +195,7 @@ bool from_built(const fcb::Built& B, const fcb::Tables& T, Molecule& M, std::str
     M.neighs = B.neighs; M.REQ = B.REQ;
     M.apars = B.apars; M.bLs = B.bLs; M.bKs = B.bKs; M.Ksp = B.Ksp; M.Kpp = B.Kpp;
     if (B.pbc) M.neighCell = B.neighCell;
+    M.permut = B.permut;
     M.bkneighs.assign(4 * (size_t)B.natoms, -1);
     for (int ia = 0; ia < B.nnode; ia++) for (int j = 0; j < 4; j++) {   // MMFFsp3_loc::makeBackNeighs
         const int ja = M.neighs[4 * ia + j];
@@ -232,6 +235,10 @@ struct LegacyWorld {
     int flags = 1 | 2 | 4 | 8 | 16 | 128 | 256 | 512;
     bool bGrid = false;
     bool fc_tables = false;       // FireCore's tables were found and typed the molecule
+    // Constrains of the world (addDistConstrain / addAngConstrain), the same for every replica:
+    // dist rows (i0, i1 | lmin, lmax, kmin, kmax, flim, shift a, b, c), angle rows (centre, end1, end2 | ang0, k)
+    std::vector<int> dist_i, ang_i;
+    std::vector<double> dist_p, ang_p;
     fcb::Tables tables;
     // FIRE (set_opt) -- pyBall/MMFF_multi.py:349 defaults
     double fire[9] = {0.1, 0.02, 0.2, 1.1, 0.5, 0.8, 5, 0.0, 10.0};
@@ -266,6 +273,8 @@ LegacyWorld L;
 int nvecs() { return L.mol.natoms + L.mol.nnode; }
 
 void set_error(const std::string& m) { mmff_set_error(m.c_str()); if (g_verbosity >= 0) fprintf(stderr, "MMFFmulti_lib: %s\n", m.c_str()); }
+
+int push_bond_constraints();
 
 // pack the CSR arrays of nSys replicas from the mirrors and upload them
 int upload_all(bool params) {
@@ -303,7 +312,20 @@ int upload_all(bool params) {
     bool any = false;
     for (size_t i = 0; i < ca.size(); i++) { ca[i] = L.constr[i]; ck[i] = L.constrK[i]; }
     for (size_t i = 0; i < (size_t)ns * na; i++) any |= ca[4 * i + 3] > 0 && (ck[4 * i] > 0 || ck[4 * i + 1] > 0 || ck[4 * i + 2] > 0);
-    return mmff_set_constraints(any ? ca.data() : nullptr, any ? ck.data() : nullptr);
+    if (mmff_set_constraints(any ? ca.data() : nullptr, any ? ck.data() : nullptr)) return -1;
+    return push_bond_constraints();
+}
+
+// the world's distance / angle constraints to the device, for every replica.
+// FireCore applies its Constrains only once a distance constraint switched
+// bConstrains on (libMMFF.h:41-47: addAngConstrain alone does not)
+int push_bond_constraints() {
+    const int nd = (int)L.dist_i.size() / 2, nang = nd ? (int)L.ang_i.size() / 3 : 0;
+    if (!nd) return mmff_set_bond_constraints(0, nullptr, nullptr, 0, nullptr, nullptr);
+    std::vector<int> di(3 * (size_t)nd), ai(4 * (size_t)nang);
+    for (int c = 0; c < nd; c++) { di[3 * c] = -1; di[3 * c + 1] = L.dist_i[2 * c]; di[3 * c + 2] = L.dist_i[2 * c + 1]; }
+    for (int c = 0; c < nang; c++) { ai[4 * c] = -1; for (int k = 0; k < 3; k++) ai[4 * c + 1 + k] = L.ang_i[3 * c + k]; }
+    return mmff_set_bond_constraints(nd, di.data(), L.dist_p.data(), nang, ai.data(), L.ang_p.data());
 }
 
 // device state -> mirrors
@@ -416,6 +438,7 @@ void* init(int nSys, char* xyz_name, char* surf_name, char* smile_name, bool bMM
            int nExplore, int nRelax, double pos_kick, double vel_kick, int GridFF) {
     (void)smile_name; (void)bMMFF; (void)nExplore; (void)nRelax; (void)pos_kick; (void)vel_kick;
     L.T = T; L.gamma = gamma; L.md_set = false;
+    L.dist_i.clear(); L.dist_p.clear(); L.ang_i.clear(); L.ang_p.clear();
     {   // a new world: the cell of an earlier init (its substrate or xyz) does not carry over
         const double lv0[9] = {20, 0, 0, 0, 20, 0, 0, 0, 20};
         memcpy(L.lvec, lv0, sizeof L.lvec);
@@ -784,13 +807,32 @@ double eval() {
     return E;
 }
 
+// libMMFF.h:41-47 (MolWorld_sp3::addDistConstrain, MolWorld_sp3.h:515-521): a
+// flat-bottom spring between atoms i0 and i1 of every replica, applied by the
+// relaxations from the next run on.  bOldIndex: i0, i1 count atoms in the
+// input order (before nodes were sorted first), as the reference's
+// builder.atom_permut maps them.
 void addDistConstrain(int i0, int i1, double lmin, double lmax, double kmin, double kmax, double flim, double* shift, bool bOldIndex) {
-    (void)i0; (void)i1; (void)lmin; (void)lmax; (void)kmin; (void)kmax; (void)flim; (void)shift; (void)bOldIndex;
-    set_error("addDistConstrain: constraints are not part of the GPU relaxation path");
+    if (!L.ready) { set_error("addDistConstrain: call init first"); return; }
+    const int nperm = (int)L.mol.permut.size();
+    if (bOldIndex) {
+        if (i0 < 0 || i1 < 0 || i0 >= nperm || i1 >= nperm) { set_error("addDistConstrain: atom index out of range"); return; }
+        i0 = L.mol.permut[i0]; i1 = L.mol.permut[i1];
+    }
+    if (i0 < 0 || i1 < 0 || i0 >= L.mol.natoms || i1 >= L.mol.natoms) { set_error("addDistConstrain: atom index out of range"); return; }
+    L.dist_i.push_back(i0); L.dist_i.push_back(i1);
+    const double sh[3] = {shift ? shift[0] : 0.0, shift ? shift[1] : 0.0, shift ? shift[2] : 0.0};
+    for (double v : {lmin, lmax, kmin, kmax, flim, sh[0], sh[1], sh[2]}) L.dist_p.push_back(v);
+    if (push_bond_constraints()) set_error(std::string("addDistConstrain: ") + mmff_last_error());
 }
+// libMMFF.h:45-47: the angle i1-i0-i2 (i0 the centre) held at ang0 with
+// E = k (1 - cos((a - ang0)/2)); active once a distance constraint exists
 void addAngConstrain(int i0, int i1, int i2, double ang0, double k) {
-    (void)i0; (void)i1; (void)i2; (void)ang0; (void)k;
-    set_error("addAngConstrain: constraints are not part of the GPU relaxation path");
+    if (!L.ready) { set_error("addAngConstrain: call init first"); return; }
+    for (int i : {i0, i1, i2}) if (i < 0 || i >= L.mol.natoms) { set_error("addAngConstrain: atom index out of range"); return; }
+    L.ang_i.push_back(i0); L.ang_i.push_back(i1); L.ang_i.push_back(i2);
+    L.ang_p.push_back(ang0); L.ang_p.push_back(k);
+    if (push_bond_constraints()) set_error(std::string("addAngConstrain: ") + mmff_last_error());
 }
 
 // manipulation of the current replica's CPU buffers (DOFs); apply with pack_system + upload

@@ -819,6 +819,7 @@ struct Engine {
                 const float3 u = f3(spos[v]);
                 f = fma3(u, -dot3(f, u), f);      // Vec3::makeOrthoU
             }
+            if ((P.flags & F_BCONS) && v < natoms) f = bond_constraint_force(Y, isys, v, spos, lv, f);
             if (P.Flim > 0.f) {
                 const float fr2 = dot3(f, f);
                 if (fr2 > Fl2) f = f * (P.Flim * rsqrtf(fr2));

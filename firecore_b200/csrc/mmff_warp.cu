@@ -574,6 +574,7 @@ struct WarpEngine {
                 if (!valid) continue;
                 float3 f = (w == 0) ? fasm_a[k] : fasm_p[k];
                 const float3 v = (w == 0) ? va[k] : vp[k];
+                if ((P.flags & F_BCONS) && w == 0) f = bond_constraint_force(Y, isys, a, sp, lv, f);
                 if (Fl > 0.f) {
                     const float fr2 = dot3(f, f);
                     if (fr2 > Fl * Fl) f = f * (Fl * rsqrtf(fr2));

@@ -113,6 +113,10 @@ struct World {
     // position springs (relax only)
     DBuf<float4> d_constr, d_constrK;
     bool has_constr = false;
+    // distance / angle constraints (mmff_set_bond_constraints)
+    DBuf<int4> d_dci, d_aci;
+    DBuf<float4> d_dca, d_dcb, d_aca;
+    int ndcon = 0, nacon = 0;
     // per-atom GridFF stencil cache of the CTA engine (grid_slice_cached)
     DBuf<unsigned int> d_gkey; DBuf<float4> d_gcs;
     bool gcache = true;            // mmff_set_grid_cache
@@ -173,6 +177,8 @@ Params make_params(bool for_eval, int nstep_max, double Fconv, int conv_mode) {
     if (excl13_active(P.flags)) P.flags |= F_EXCL13;
     P.flags &= ~F_CONSTR;
     if (W.has_constr && !for_eval) P.flags |= F_CONSTR;
+    P.flags &= ~F_BCONS;
+    if ((W.ndcon || W.nacon) && !for_eval) P.flags |= F_BCONS;
     if (!W.grid.p) P.flags &= ~F_GRID;
     for (int k = 0; k < 3; k++) P.npbc[k] = W.npbc[k];
     P.Rc2 = W.Rcut > 0 ? (float)(W.Rcut * W.Rcut) : 0.f;
@@ -211,6 +217,8 @@ Systems make_systems() {
     Y.apars = W.d_apar.p; Y.bLs = W.d_bL.p; Y.bKs = W.d_bK.p; Y.Ksp = W.d_ksp.p; Y.Kpp = W.d_kpp.p;
     Y.a13 = W.d_a13.p; Y.xmask = W.d_xmask.p; Y.moff = W.d_moff.p;
     Y.constr = W.d_constr.p; Y.constrK = W.d_constrK.p;
+    Y.dcon_i = W.d_dci.p; Y.dcon_a = W.d_dca.p; Y.dcon_b = W.d_dcb.p; Y.ndcon = W.ndcon;
+    Y.acon_i = W.d_aci.p; Y.acon_a = W.d_aca.p; Y.nacon = W.nacon;
     // the cache keys pack the stencil cell into 12 + 12 + 8 bits
     const bool gc = W.gcache && W.d_gkey.p && W.gn[0] <= 4096 && W.gn[1] <= 4096 && W.gn[2] <= 256;
     Y.gkey = gc ? W.d_gkey.p : nullptr; Y.gcs = gc ? W.d_gcs.p : nullptr;
@@ -690,6 +698,7 @@ int mmff_systems_upload(int nsys, const int* natoms, const int* nnode, const dou
         return -1;
     W.h_ng = std::move(hng); W.h_ngC = std::move(hngC); W.h_a13 = std::move(ha13);
     W.has_constr = false;           // springs belong to the systems they were set for
+    W.ndcon = 0; W.nacon = 0;       // and so do the distance / angle constraints
     if (W.d_force.ensure(NV) || W.d_energy.ensure(nsys) || W.d_status.ensure(nsys) || W.d_nsteps.ensure(nsys) ||
         W.d_fconv.ensure(nsys) || W.d_counter.ensure(64) || W.d_stats.ensure(8) || W.d_gkey.ensure(NA) ||
         W.d_gcs.ensure((size_t)NA * 16) || clear_grid_cache())
@@ -728,6 +737,51 @@ int mmff_set_constraints(const double* anchor, const double* K) {
     if (upload(W.d_constr, ha) || upload(W.d_constrK, hk)) return -1;
     CK(cudaStreamSynchronize(W.stream));
     W.has_constr = any;
+    return 0;
+}
+
+// Distance and angle constraints between atoms (FireCore's Constrains bonds /
+// angles, constrains.h), for the relax kernels.  dist_idx [ndist*3] = (system
+// or -1 for every system, i0, i1); dist_par [ndist*8] = (lmin, lmax, kmin,
+// kmax, flim, shift along a, b, c); ang_idx [nang*4] = (system or -1, centre,
+// end 1, end 2); ang_par [nang*2] = (ang0 [rad], k).  Local atom indices.
+int mmff_set_bond_constraints(int ndist, const int* dist_idx, const double* dist_par, int nang, const int* ang_idx,
+                              const double* ang_par) {
+    if (ensure_ready()) return -1;
+    if (!W.nsys) return fail("no systems uploaded");
+    if (ndist < 0 || nang < 0 || (ndist && (!dist_idx || !dist_par)) || (nang && (!ang_idx || !ang_par)))
+        return fail("mmff_set_bond_constraints: bad counts or NULL arrays");
+    auto check = [&](int sys, const int* at, int n, const char* what) -> int {
+        if (sys < -1 || sys >= W.nsys) return fail("%s constraint: system %d out of range", what, sys);
+        for (int k = 0; k < n; k++) {
+            const int lim = sys >= 0 ? W.natoms[sys] : *std::min_element(W.natoms.begin(), W.natoms.end());
+            if (at[k] < 0 || at[k] >= lim) return fail("%s constraint: atom %d out of range", what, at[k]);
+        }
+        return 0;
+    };
+    std::vector<int4> di(ndist), ai(nang);
+    std::vector<float4> da(ndist), db(ndist), aa(nang);
+    for (int c = 0; c < ndist; c++) {
+        const int* x = dist_idx + 3 * c;
+        const double* q = dist_par + 8 * c;
+        if (check(x[0], x + 1, 2, "distance")) return -1;
+        di[c] = make_int4(x[0], x[1], x[2], 0);
+        da[c] = make_float4((float)q[1], (float)q[0], (float)q[3], (float)q[2]);   // (lmax, lmin, kmax, kmin)
+        db[c] = make_float4((float)q[5], (float)q[6], (float)q[7], (float)q[4]);
+    }
+    for (int c = 0; c < nang; c++) {
+        const int* x = ang_idx + 4 * c;
+        const double* q = ang_par + 2 * c;
+        if (check(x[0], x + 1, 3, "angle")) return -1;
+        ai[c] = make_int4(x[0], x[1], x[2], x[3]);
+        aa[c] = make_float4((float)cos(q[0] * 0.5), (float)sin(q[0] * 0.5), (float)q[1], 0.f);
+    }
+    W.version++;
+    W.ndcon = 0; W.nacon = 0;
+    if (ndist && (upload(W.d_dci, di) || upload(W.d_dca, da) || upload(W.d_dcb, db))) return -1;
+    if (nang && (upload(W.d_aci, ai) || upload(W.d_aca, aa))) return -1;
+    CK(cudaStreamSynchronize(W.stream));
+    W.ndcon = ndist; W.nacon = nang;
     return 0;
 }
 

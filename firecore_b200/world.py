@@ -168,6 +168,20 @@ class World:
         k = np.zeros((a.shape[0], 4)); k[:, :np.asarray(K).shape[1]] = K
         _check(self.lib.mmff_set_constraints(_lib.ptr(a), _lib.ptr(k)), "mmff_set_constraints")
 
+    def set_bond_constraints(self, dist=(), angles=()):
+        """Distance / angle constraints between atoms for relaxations (FireCore's
+        Constrains, constrains.h): dist = [(system or -1, i0, i1, lmin, lmax, kmin,
+        kmax, flim[, sa, sb, sc])], angles = [(system or -1, centre, end1, end2,
+        ang0_rad, k)]; local atom indices; empty clears."""
+        di = np.array([[int(x) for x in d[:3]] for d in dist], np.int32).reshape(-1, 3)
+        dp = np.zeros((len(dist), 8))
+        for r, d in enumerate(dist):
+            dp[r, :len(d) - 3] = d[3:]
+        ai = np.array([[int(x) for x in a[:4]] for a in angles], np.int32).reshape(-1, 4)
+        ap = np.array([a[4:6] for a in angles], np.float64).reshape(-1, 2)
+        _check(self.lib.mmff_set_bond_constraints(len(dist), _lib.ptr(di), _lib.ptr(dp), len(angles), _lib.ptr(ai),
+                                                  _lib.ptr(ap)), "mmff_set_bond_constraints")
+
     def restore(self):
         _check(self.lib.mmff_systems_restore(), "mmff_systems_restore")
 

@@ -116,6 +116,21 @@ int mmff_systems_upload(int nsys, const int* natoms, const int* nnode, const dou
  * atom's force after the force clamp.  mmff_eval reports forces without
  * them.  anchor NULL clears; mmff_systems_upload clears. */
 int mmff_set_constraints(const double* anchor, const double* K);
+/* Distance and angle constraints between atoms for relaxations (FireCore's
+ * Constrains: DistConstr / AngleConstr, cpp/common/molecular/constrains.h:83-146;
+ * added by addDistConstrain / addAngConstrain, libMMFF.h:41-47, applied by
+ * MolWorld_sp3::run_no_omp after the force field, MolWorld_sp3.h:2391-2395).
+ * dist_idx [ndist*3] = (system, or -1 for every system; i0; i1) local atom
+ * indices; dist_par [ndist*8] = (lmin, lmax, kmin, kmax, flim, shift along the
+ * cell vectors a, b, c): a flat-bottom spring on |p[i1] - p[i0] + shift| with
+ * constant kmax above lmax and kmin below lmin, its force capped at flim
+ * (Forces.h:161 spring).  ang_idx [nang*4] = (system or -1, centre, end 1,
+ * end 2); ang_par [nang*2] = (ang0 [rad], k): E = k (1 - cos((a - ang0)/2))
+ * (evalAngleCosHalf).  The forces join each atom's force before the force
+ * clamp; mmff_eval reports forces without them.  ndist = nang = 0 clears;
+ * mmff_systems_upload clears. */
+int mmff_set_bond_constraints(int ndist, const int* dist_idx, const double* dist_par, int nang, const int* ang_idx,
+                              const double* ang_par);
 /* No counterpart in the reference.  Per-atom cache of the 64 channel-combined
  * B-spline coefficients (PLQ . C) of the atom's GridFF stencil in the CTA
  * relax kernels: on (1, default) an atom re-gathers the grid only when its

@@ -508,6 +508,50 @@ void orc_eval(int nsys, const int* natoms, const int* nnode,
     free_offsets(o);
 }
 
+/* Constrains::apply (constrains.h:386-394) for system s: DistConstr::apply
+ * (:95-109) with Forces.h:161 spring, AngleConstr::apply (:123-144) with
+ * evalAngleCosHalf (Forces.h:190-215), cells of the angle arms zero.  p, f:
+ * the system's positions and forces [nvecs*3]; lv: its cell rows a, b, c. */
+static void bond_constraints(int s, const double* p, double* f, const double* lv, int ndist, const int* di,
+                             const double* dp, int nang, const int* ai, const double* ap) {
+    for (int c = 0; c < ndist; c++) {
+        const int* x = di + 3 * c;
+        const double* q = dp + 8 * c;   /* lmin, lmax, kmin, kmax, flim, shift */
+        if (x[0] >= 0 && x[0] != s) continue;
+        const int i0 = x[1], i1 = x[2];
+        double d[3];
+        for (int k = 0; k < 3; k++) d[k] = p[3 * i1 + k] - p[3 * i0 + k] + (lv[k] * q[5] + lv[3 + k] * q[6] + lv[6 + k] * q[7]);
+        const double l = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+        double fs = 0;
+        if (l > q[1]) { fs = (l - q[1]) * q[3]; if (fs > q[4]) fs = q[4]; }
+        else if (l < q[0]) { fs = (l - q[0]) * q[2]; if (fs < -q[4]) fs = -q[4]; }
+        for (int k = 0; k < 3; k++) { const double g = d[k] * (fs / l); f[3 * i1 + k] -= g; f[3 * i0 + k] += g; }
+    }
+    for (int c = 0; c < nang; c++) {
+        const int* x = ai + 4 * c;
+        if (x[0] >= 0 && x[0] != s) continue;
+        const int ic = x[1], ia = x[2], ib = x[3];
+        double h1[3], h2[3], h[3];
+        for (int k = 0; k < 3; k++) { h1[k] = p[3 * ic + k] - p[3 * ia + k]; h2[k] = p[3 * ic + k] - p[3 * ib + k]; }
+        const double l1 = sqrt(h1[0] * h1[0] + h1[1] * h1[1] + h1[2] * h1[2]);
+        const double l2 = sqrt(h2[0] * h2[0] + h2[1] * h2[1] + h2[2] * h2[2]);
+        const double ir1 = 1. / l1, ir2 = 1. / l2;
+        for (int k = 0; k < 3; k++) { h1[k] *= ir1; h2[k] *= ir2; h[k] = h1[k] + h2[k]; }
+        double c2 = (h[0] * h[0] + h[1] * h[1] + h[2] * h[2]) * 0.25;
+        const double s2 = 1 - c2 + 1e-14, cc = sqrt(c2), ss = sqrt(s2);
+        const double c0 = cos(ap[2 * c] * 0.5), s0 = sin(ap[2 * c] * 0.5), kk = ap[2 * c + 1];
+        const double csy = s0 * cc - c0 * ss;
+        double fr = -kk * csy;
+        c2 *= -2;
+        fr /= 4 * cc * ss;
+        const double fr1 = fr * ir1, fr2 = fr * ir2;
+        for (int k = 0; k < 3; k++) {
+            const double f1 = h[k] * fr1 + h1[k] * (fr1 * c2), f2 = h[k] * fr2 + h2[k] * (fr2 * c2);
+            f[3 * ia + k] -= f1; f[3 * ic + k] += f1 + f2; f[3 * ib + k] -= f2;
+        }
+    }
+}
+
 /* DynamicOpt.cpp:250-267 FIRE_update_params, then MMFFsp3_loc.h:1264-1281
  * move_atom_FIRE for every vector, as called from MolWorld_sp3::run_no_omp
  * (MolWorld_sp3.h:2401-2430): move_atom_FIRE(i, (float)opt.dt, 1e4, opt.cv,
@@ -520,7 +564,9 @@ void orc_relax(int nsys, const int* natoms, const int* nnode,
                const double* lvec, const double* gridC, const ORC_params* P,
                const ORC_fire* F, int niter, double Fconv, int conv_mode,
                int* nsteps_out, int* conv_out, double* Fout, double* Eout, int nthreads,
-               const double* constr, const double* constrK) {
+               const double* constr, const double* constrK,
+               int ndist, const int* dist_idx, const double* dist_par,
+               int nang, const int* ang_idx, const double* ang_par) {
     offsets_t o = make_offsets(nsys, natoms, nnode);
     size_t nvtot = (size_t)o.voff[nsys];
     double* force = (double*)calloc(nvtot * 3 + 3, sizeof(double));
@@ -545,6 +591,7 @@ void orc_relax(int nsys, const int* natoms, const int* nnode,
         const int nv = S.nvecs;
         for (itr = 0; itr < niter; itr++) {
             eval_system(&S, P, gridC, Ep);
+            if (ndist || nang) bond_constraints(s, p, S.force, lvec + 9 * s, ndist, dist_idx, dist_par, nang, ang_idx, ang_par);
             if (F->Flim > 0) {
                 const double Fl2 = F->Flim * F->Flim;
                 for (int i = 0; i < nv; i++) {

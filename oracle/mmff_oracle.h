@@ -83,6 +83,11 @@ void orc_eval(int nsys, const int* natoms, const int* nnode,
               int nthreads);
 
 /* FIRE relaxation of every system, MolWorld_sp3::run_no_omp semantics.
+ * Distance / angle constraints (optional, ndist / nang = 0: none):
+ * dist_idx [ndist*3] = (system or -1 = all, i0, i1), dist_par [ndist*8] =
+ * (lmin, lmax, kmin, kmax, flim, shift a, b, c); ang_idx [nang*4] = (system or
+ * -1, centre, end 1, end 2), ang_par [nang*2] = (ang0 rad, k); applied after
+ * the force field and before the clamp (MolWorld_sp3.h:2391-2395).
  * fire_state[s*4]: dt, damping, lastNeg (as double), unused.
  * conv_mode 0: sum_DOF f^2 < Fconv^2 (reference); 1: max_vec |f| < Fconv.
  * nsteps_out[s]: steps done (the reference's return value), conv_out[s]:
@@ -95,7 +100,9 @@ void orc_relax(int nsys, const int* natoms, const int* nnode,
                const double* lvec, const double* gridC, const ORC_params* P,
                const ORC_fire* F, int niter, double Fconv, int conv_mode,
                int* nsteps_out, int* conv_out, double* Fout, double* Eout,
-               int nthreads, const double* constr, const double* constrK);
+               int nthreads, const double* constr, const double* constrK,
+               int ndist, const int* dist_idx, const double* dist_par,
+               int nang, const int* ang_idx, const double* ang_par);
 
 /* Langevin dynamics, MMFFsp3_loc::move_atom_Langevin (MMFFsp3_loc.h:1191-1216):
  * per step and vector f -= gamma v; f += u sqrt(2 kB T gamma / dt) with u in

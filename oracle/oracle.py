@@ -146,11 +146,12 @@ def eval_forces(b, P: ORCParams, gridC=None, pos=None, nthreads=0):
 
 
 def relax(b, P: ORCParams, F: ORCFire, gridC=None, niter=1000, Fconv=1e-4, conv_mode=0, pos=None, vel=None,
-          fire_state=None, nthreads=0, constr=None, constrK=None):
+          fire_state=None, nthreads=0, constr=None, constrK=None, dist=(), angles=()):
     """FIRE relaxation (run_no_omp semantics). Returns dict of arrays.
     constr / constrK [sum natoms, 4] (optional): per-atom position springs,
     anchor (x, y, z, on if w > 0) and constants (kx, ky, kz, -) in the same
-    frame as pos."""
+    frame as pos.  dist / angles: distance and angle constraints as
+    World.set_bond_constraints takes them."""
     lib = orc()
     pos = np.array(b.pos if pos is None else pos, np.float64, order="C")
     vel = np.zeros_like(pos) if vel is None else np.array(vel, np.float64, order="C")
@@ -164,12 +165,18 @@ def relax(b, P: ORCParams, F: ORCFire, gridC=None, niter=1000, Fconv=1e-4, conv_
     keep = [np.ascontiguousarray(b.natoms, np.int32), np.ascontiguousarray(b.nnode, np.int32)]
     g = None if gridC is None else np.ascontiguousarray(gridC, np.float64)
     arrs = _sysarrays(b)
+    di = np.array([[int(x) for x in d[:3]] for d in dist], np.int32).reshape(-1, 3)
+    dp = np.zeros((len(dist), 8))
+    for r, d in enumerate(dist):
+        dp[r, :len(d) - 3] = d[3:]
+    ai = np.array([[int(x) for x in a[:4]] for a in angles], np.int32).reshape(-1, 4)
+    ap = np.array([a[4:6] for a in angles], np.float64).reshape(-1, 2)
     cs = None if constr is None else np.ascontiguousarray(constr, np.float64)
     ck = None if constrK is None else np.ascontiguousarray(constrK, np.float64)
     lib.orc_relax(ctypes.c_int(b.nsys), _p(keep[0]), _p(keep[1]), _p(pos), _p(vel), _p(fire_state), *[_p(a) for a in arrs],
                   _p(g), ctypes.byref(P), ctypes.byref(F), ctypes.c_int(niter), ctypes.c_double(Fconv),
                   ctypes.c_int(conv_mode), _p(nsteps), _p(conv), _p(Fout), _p(Eout), ctypes.c_int(nthreads),
-                  _p(cs), _p(ck))
+                  _p(cs), _p(ck), ctypes.c_int(len(dist)), _p(di), _p(dp), ctypes.c_int(len(angles)), _p(ai), _p(ap))
     return dict(pos=pos, vel=vel, fire_state=fire_state, nsteps=nsteps, converged=conv, F=Fout, E=Eout)
 
 
@@ -211,8 +218,8 @@ def langevin_rand(seed, vec, step, comp):
 def grid_sample(pos, PLQ, gridC, P: ORCParams):
     pos = np.ascontiguousarray(pos, np.float64); PLQ = np.ascontiguousarray(PLQ, np.float64)
     fe = np.zeros((pos.shape[0], 4))
-    orc().orc_grid_sample(ctypes.c_int(pos.shape[0]), _p(pos), _p(PLQ), _p(np.ascontiguousarray(gridC, np.float64)),
-                          ctypes.byref(P), _p(fe))
+    C = np.ascontiguousarray(gridC, np.float64)      # held for the duration of the call
+    orc().orc_grid_sample(ctypes.c_int(pos.shape[0]), _p(pos), _p(PLQ), _p(C), ctypes.byref(P), _p(fe))
     return fe
 
 
@@ -229,8 +236,9 @@ def grid_potentials(sub, nthreads=0):
     nx, ny, nz = sub.grid.n
     V = np.zeros((nx, ny, nz, 3))
     nm = np.array(sub.nPBC_mors, np.int32); nc = np.array(sub.nPBC_coul, np.int32)
-    orc().orc_grid_potentials(ctypes.c_int(sub.spos.shape[0]), _p(np.ascontiguousarray(sub.spos)),
-                              _p(np.ascontiguousarray(sub.sREQ)), _p(np.ascontiguousarray(sub.lvec.reshape(9))),
+    sp = np.ascontiguousarray(sub.spos, np.float64); sq = np.ascontiguousarray(sub.sREQ, np.float64)
+    lv = np.ascontiguousarray(sub.lvec.reshape(9), np.float64)   # held for the duration of the call
+    orc().orc_grid_potentials(ctypes.c_int(sub.spos.shape[0]), _p(sp), _p(sq), _p(lv),
                               _p(nm), _p(nc), ctypes.byref(P), _p(V), ctypes.c_int(nthreads))
     return V
 

@@ -151,6 +151,26 @@ int ref_relax(int niter, double Fconv, double* pos, double* vel, double* fire, d
     return itr;
 }
 
+// Distance / angle constraints of the current system (after ref_setup), as
+// MolWorld_sp3::addDistConstrain (MolWorld_sp3.h:515-521) and libMMFF.h:45-47
+// add them; run_no_omp applies them when bConstrains is on.  dp rows: lmin,
+// lmax, kmin, kmax, flim, shift a, b, c; ap rows: ang0, k.  The angle arms'
+// cells, which AngleConstr's constructor leaves unset, are zero.
+void ref_set_constraints(int nd, const int* di, const double* dp, int na, const int* ai, const double* ap) {
+    W.constrs.bonds.clear();
+    W.constrs.angles.clear();
+    for (int c = 0; c < nd; c++) {
+        const double* q = dp + 8 * c;
+        W.addDistConstrain(di[2 * c], di[2 * c + 1], q[0], q[1], q[2], q[3], q[4], Vec3d{q[5], q[6], q[7]}, false);
+    }
+    for (int c = 0; c < na; c++) {
+        AngleConstr a(Vec3i{ai[3 * c], ai[3 * c + 1], ai[3 * c + 2]}, Vec2d{cos(ap[2 * c] / 2.), sin(ap[2 * c] / 2.)}, ap[2 * c + 1]);
+        a.acell = Vec3iZero; a.bcell = Vec3iZero;
+        W.constrs.angles.push_back(a);
+    }
+    W.bConstrains = nd > 0;
+}
+
 void ref_grid_sample(int n, const double* pos, const double* PLQ, double* fe) {
     for (int i = 0; i < n; i++) {
         Quat4d r = W.gridFF.getForce_Bspline(Vec3d{pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]},

@@ -51,8 +51,9 @@ def _ref_child(xyz, epairs, out):
     par = [np.zeros((cap, 4)) for _ in range(5)]
     names = ctypes.create_string_buffer(8 * cap)
     P = lambda a: ctypes.c_void_p(a.ctypes.data)  # noqa: E731
+    npbc = np.array(NPBC, np.int32)                 # held for the duration of the call
     n = lib.ref_build_xyz(*(os.path.join(RES, t).encode() for t in TABLES), xyz.encode(), ctypes.c_int(epairs),
-                          P(np.array(NPBC, np.int32)), ctypes.c_int(cap), P(cnt), P(apos), P(REQ), P(at), P(ng), P(nc),
+                          P(npbc), ctypes.c_int(cap), P(cnt), P(apos), P(REQ), P(at), P(ng), P(nc),
                           *[P(a) for a in par], names)
     na, nn = int(cnt[0]), int(cnt[1])
     d = dict(natoms=na, nnode=nn, pbc=int(cnt[3]), apos=apos[:na + nn], REQs=REQ[:na], neighs=ng[:na],

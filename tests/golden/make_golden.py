@@ -103,18 +103,20 @@ def main():
     REQ = np.stack([rng.uniform(1.5, 2.0, 64), np.sqrt(rng.uniform(0.002, 0.01, 64)), rng.normal(0, 0.3, 64),
                     np.zeros(64)], 1)
     PLQ = np.zeros_like(REQ)
-    ref.ref_req2plq(64, p(np.ascontiguousarray(REQ)), ctypes.c_double(1.5), p(PLQ))
+    REQ = np.ascontiguousarray(REQ); pts = np.ascontiguousarray(pts)
+    ref.ref_req2plq(64, p(REQ), ctypes.c_double(1.5), p(PLQ))
     fe = np.zeros((64, 4))
-    ref.ref_grid_sample(64, p(np.ascontiguousarray(pts)), p(PLQ), p(fe))
+    ref.ref_grid_sample(64, p(pts), p(PLQ), p(fe))
     out.update(samp_pos=pts, samp_REQ=REQ, samp_PLQ=PLQ, samp_fe=fe)
     # grid-node potentials at a few nodes
     idx = rng.integers(0, [g.n[0], g.n[1], g.n[2]], size=(16, 3))
     pts2 = np.stack([g.pos0[k] + g.step[k] * idx[:, k] for k in range(3)], 1)
     Vp = np.zeros((16, 3))
-    ref.ref_grid_points(16, p(np.ascontiguousarray(pts2)), sub.spos.shape[0], p(np.ascontiguousarray(sub.spos)),
-                        p(np.ascontiguousarray(sub.sREQ)), p(np.ascontiguousarray(sub.lvec.reshape(9))),
-                        p(np.array(sub.nPBC_mors, np.int32)), p(np.array(sub.nPBC_coul, np.int32)),
-                        ctypes.c_double(1.5), p(Vp))
+    # arrays held in names for the duration of each native call
+    pts2 = np.ascontiguousarray(pts2); sp = np.ascontiguousarray(sub.spos); sq = np.ascontiguousarray(sub.sREQ)
+    lv = np.ascontiguousarray(sub.lvec.reshape(9))
+    nm = np.array(sub.nPBC_mors, np.int32); nc = np.array(sub.nPBC_coul, np.int32)
+    ref.ref_grid_points(16, p(pts2), sub.spos.shape[0], p(sp), p(sq), p(lv), p(nm), p(nc), ctypes.c_double(1.5), p(Vp))
     out.update(node_idx=idx, node_V=Vp)
     # Bspline::fit3D_omp on a small smooth periodic-in-xy grid (x-fastest order)
     nsx, nsy, nsz = 8, 10, 12
@@ -123,7 +125,8 @@ def main():
     Ef = np.cos(2 * np.pi * xs) * np.sin(2 * np.pi * ys) * np.exp(-2 * zs) + 0.3 * np.cos(4 * np.pi * (xs + ys)) * zs
     Ef = np.ascontiguousarray(Ef + 0 * zs)
     Gf = np.zeros_like(Ef)
-    nit = ref.ref_fit3d(p(np.array([nsx, nsy, nsz], np.int32)), p(Ef), p(Gf), ctypes.c_double(1e-13), 200000,
+    ns = np.array([nsx, nsy, nsz], np.int32)
+    nit = ref.ref_fit3d(p(ns), p(Ef), p(Gf), ctypes.c_double(1e-13), 200000,
                         ctypes.c_double(0.3))
     out.update(fit_E=Ef, fit_G=Gf, fit_niter=np.array(nit))
     np.savez_compressed(OUT, **out)

@@ -86,3 +86,30 @@ def test_legacy_init_types_with_firecore_tables(tmp_path, monkeypatch):
     n = mmff.run(nstepMax=2000, Fconv=1e-3)
     assert 0 < n <= 2000 and np.isfinite(mmff.gpu_atoms).all()
     assert mmff.eval() < E
+
+
+def test_legacy_distance_and_angle_constraints(tmp_path, monkeypatch):
+    """addDistConstrain / addAngConstrain (libMMFF.h:41-47) act on every
+    replica in the next run, as FireCore's default run path applies its
+    Constrains to all replicas."""
+    from firecore_b200 import MMFF_multi as mmff
+    monkeypatch.chdir(tmp_path)                       # no FireCore tables here: the library's own table
+    mmff.init(nSys_=4, xyz_name=os.path.join(HERE, "mol24.xyz"), nPBC=(1, 1, 0))
+    mmff.getBuffs()
+    p0 = mmff.gpu_atoms[:, :24, :3].copy()
+    d0 = np.linalg.norm(p0[:, 0] - p0[:, 9], axis=1)
+    mmff.set_opt(dt_max=0.05, dt_min=0.005, damp_max=0.1, minLastNeg=3)
+    # relaxed without constraints
+    mmff.run(nstepMax=3000, Fconv=1e-3)
+    free = np.linalg.norm(mmff.gpu_atoms[:, 0, :3] - mmff.gpu_atoms[:, 9, :3], axis=1)
+    # again from the start, atoms 0 and 9 held 1 A further apart
+    mmff.gpu_atoms[:, :24, :3] = p0
+    mmff.gpu_avel[:] = 0
+    mmff.upload(bParams=False, bForces=False, bVel=True)
+    mmff.addDistConstrain(0, 9, l=float(d0[0]) + 1.0, k=5.0, flim=20.0)
+    mmff.addAngConstrain(1, 0, 2, ang0=2.0, k=0.5)
+    mmff.run(nstepMax=3000, Fconv=1e-3)
+    held = np.linalg.norm(mmff.gpu_atoms[:, 0, :3] - mmff.gpu_atoms[:, 9, :3], axis=1)
+    assert np.isfinite(mmff.gpu_atoms).all()
+    assert (held > free + 0.3).all(), (held, free)
+    assert np.abs(held - held[0]).max() < 1e-3        # the same on every replica

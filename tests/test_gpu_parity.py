@@ -334,3 +334,57 @@ def test_position_springs_vs_oracle(world, golden):
     _, Eg = O.eval_forces(b, O.make_params(grid), golden["C"], pos=st["pos"])
     _, Ec = O.eval_forces(b, O.make_params(grid), golden["C"], pos=r["pos"])
     assert (np.abs(Eg[:, 3] - Ec[:, 3]) / b.natoms).max() <= 1e-5
+
+
+@pytest.mark.parametrize("threads", [0, 64])
+def test_bond_constraints_vs_oracle(world, golden, threads):
+    """Distance / angle constraints (FireCore's Constrains, constrains.h) in both
+    relax engines (threads 0: the warp-per-system kernel for these 24-atom
+    systems; 64: the CTA kernel), with three atoms per system held by position
+    springs so that every system converges: relaxed geometries match the FP64
+    oracle with the same constraints (the oracle's are pinned to FireCore's
+    run_no_omp in test_oracle_golden.py), and eval reports forces without them."""
+    grid = grid_from_golden(golden)
+    b = S.make_systems([24] * 8, seed=5, topo_mode=0, sigma=0.05, rotate=False, cell=(11.28, 11.28, 40.0))
+    dist = [(-1, 3, 12, 5.0, 5.2, 2.0, 2.0, 3.0), (3, 2, 17, 2.6, 2.8, 1.0, 1.0, 10.0, 0.0, 0.0, 0.0)]
+    ang = [(-1, 1, 0, 2, 2.4, 1.5)]
+    world.set_params(flags=DEFAULT_FLAGS)
+    world.set_fire(FireParams(Flim=10.0))
+    world.set_launch(threads=threads)
+    a, n, v = b.offsets()
+    try:
+        world.upload(b)
+        pos0 = world.state()["pos"]
+        anchor = np.zeros((int(b.natoms.sum()), 4)); anchor[:, 3] = -1.0
+        K = np.zeros((int(b.natoms.sum()), 4))
+        for s in range(b.nsys):
+            for ia in (0, 7, 17):
+                anchor[a[s] + ia, :3] = pos0[v[s] + ia]; anchor[a[s] + ia, 3] = 1.0; K[a[s] + ia, :3] = 1.0
+        world.set_constraints(anchor, K)
+        world.set_bond_constraints(dist, ang)
+        F0, _ = world.eval(False)
+        Fo0, _ = O.eval_forces(b, O.make_params(grid), golden["C"], pos=pos0)
+        assert np.abs(F0 - Fo0).max() <= 1e-5 * np.abs(Fo0).max()         # eval: no constraints
+        world.relax(6000, 1e-4, conv_mode=1)
+        st = world.state()
+        world.set_bond_constraints()
+        world.set_constraints(None)
+    finally:
+        world.set_fire(FireParams())
+        world.set_launch(0)
+    P, F = O.make_params(grid), O.make_fire(Flim=10.0)
+    r = O.relax(b, P, F, golden["C"], niter=6000, Fconv=1e-4, conv_mode=1, pos=pos0, constr=anchor, constrK=K,
+                dist=dist, angles=ang)
+    r0 = O.relax(b, P, F, golden["C"], niter=6000, Fconv=1e-4, conv_mode=1, pos=pos0, constr=anchor, constrK=K)
+    assert (st["status"] == 1).all() and (r["converged"] == 1).all()
+    for s in range(b.nsys):
+        na = b.natoms[s]
+        d = st["pos"][v[s]:v[s] + na] - r["pos"][v[s]:v[s] + na]
+        assert np.sqrt((d ** 2).sum(1).mean()) <= 1e-2, s
+        # the constraints change the result (the unconstrained minimum is elsewhere)
+        d0 = r0["pos"][v[s]:v[s] + na] - r["pos"][v[s]:v[s] + na]
+        assert np.sqrt((d0 ** 2).sum(1).mean()) > 0.1, s
+    # system 3 alone carries the second distance constraint
+    l_gpu = np.linalg.norm(st["pos"][v[3] + 2] - st["pos"][v[3] + 17])
+    l_orc = np.linalg.norm(r["pos"][v[3] + 2] - r["pos"][v[3] + 17])
+    assert abs(l_gpu - l_orc) < 1e-2

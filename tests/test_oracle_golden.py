@@ -66,3 +66,50 @@ def test_oracle_grid_potentials_reproduce_golden(golden):
     V = O.grid_potentials(sub)
     assert np.abs(V - golden["V"]).max() <= 1e-12 * np.abs(golden["V"]).max()
     assert np.abs(O.bspline_fit(V) - golden["C"]).max() <= 1e-10 * np.abs(golden["C"]).max()
+
+
+# distance / angle constraints of the test below: (i0, i1, lmin, lmax, kmin, kmax, flim, shift a, b, c)
+# and (centre, end 1, end 2, ang0, k); the second distance spring reaches into the next cell
+DIST = [(0, 5, 2.0, 2.2, 1.5, 0.8, 3.0, 0.0, 0.0, 0.0), (2, 9, 12.0, 12.5, 0.6, 0.6, 0.5, 1.0, 0.0, 0.0)]
+ANG = [(1, 0, 2, 2.0, 0.7)]
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference harness not built (FireCore tree absent)")
+def test_constraints_match_reference_run_no_omp(golden):
+    """The oracle's distance / angle constraints against FireCore's own
+    Constrains::apply inside MolWorld_sp3::run_no_omp, run live through the
+    reference harness: 300 FIRE steps of one golden molecule."""
+    import ctypes
+    b = batch_from_golden(golden, "A").subset([0])
+    g = grid_from_golden(golden)
+    flags = FLAGSETS["nogrid"]
+    na, nn = int(b.natoms[0]), int(b.nnode[0])
+    ref = O.ref()
+    ref.ref_set_constraints.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                        ctypes.c_void_p]
+    p = lambda a: ctypes.c_void_p(a.ctypes.data)  # noqa: E731
+    pos = np.ascontiguousarray(b.pos)
+    arr = [np.ascontiguousarray(x) for x in (b.neighs, b.neighCell, b.REQs)]
+    nar = [np.ascontiguousarray(x) for x in (b.apars, b.bLs, b.bKs, b.Ksp, b.Kpp)]
+    lv = np.ascontiguousarray(b.lvec[0].reshape(9))
+    npbc = np.array([1, 1, 0], np.int32)
+    gn = np.array(g.n, np.int32); gp0 = np.array(g.pos0); gst = np.array(g.step)
+    bk = np.zeros((na, 4), np.int32); ng = np.zeros((na, 4), np.int32)
+    C = np.ascontiguousarray(golden["C"])           # held: the harness reads it during the call
+    ref.ref_setup(na, nn, p(pos), p(arr[0]), p(arr[1]), p(arr[2]), *[p(x) for x in nar], p(lv), p(npbc), flags, 1.5,
+                  p(gn), p(gp0), p(gst), p(C), p(bk), p(ng))
+    di = np.array([d[:2] for d in DIST], np.int32); dp = np.array([d[2:] for d in DIST], np.float64)
+    ai = np.array([a[:3] for a in ANG], np.int32); ap = np.array([a[3:] for a in ANG], np.float64)
+    ref.ref_set_constraints(len(DIST), p(di), p(dp), len(ANG), p(ai), p(ap))
+    nit = 300
+    pr = pos.copy(); vr = np.zeros_like(pr)
+    fr = np.array([0.1, 0.1, 0.0, 0.1, 0.01, 0.1, 1.1, 0.5, 0.8, 3, 0.0])
+    oE = np.zeros(nit); oF = np.zeros(nit)
+    it = ref.ref_relax(nit, 1e-9, p(pr), p(vr), p(fr), p(oE), p(oF))
+    r = O.relax(b, O.make_params(g, flags=flags), O.make_fire(), golden["C"], niter=nit, Fconv=1e-9, conv_mode=0,
+                dist=[(-1,) + d for d in DIST], angles=[(-1,) + a for a in ANG])
+    assert int(r["nsteps"][0]) == it
+    assert np.abs(r["pos"] - pr).max() < 1e-9
+    # and the constraints act: without them the trajectory differs
+    r0 = O.relax(b, O.make_params(g, flags=flags), O.make_fire(), golden["C"], niter=nit, Fconv=1e-9, conv_mode=0)
+    assert np.abs(r0["pos"] - pr).max() > 1e-3
