@@ -178,7 +178,7 @@ def run_ours(args):
     # counting pass (untimed): algorithmic work of one relaxation of this batch
     lib.mmff_set_counting(1)
     w.restore(); w.relax(MAXSTEPS, FCONV, 1)
-    cnt = (np.ctypeslib.ctypes.c_ulonglong * 3)()
+    cnt = (np.ctypeslib.ctypes.c_ulonglong * 5)()
     lib.mmff_get_counters(np.ctypeslib.ctypes.cast(cnt, np.ctypeslib.ctypes.c_void_p))
     pair_images, grid_samples, force_evals = int(cnt[0]), int(cnt[1]), int(cnt[2])
     lib.mmff_set_counting(0)
@@ -342,7 +342,7 @@ def term_attribution(w, lib, nsteps=200):
     w.set_params(flags=DEFAULT_FLAGS, npbc=(1, 1, 0), Rcut=RCUT)
     lib.mmff_set_counting(1)
     w.restore(); w.relax(nsteps, 0.0, 1)
-    cnt = (np.ctypeslib.ctypes.c_ulonglong * 3)()
+    cnt = (np.ctypeslib.ctypes.c_ulonglong * 5)()
     lib.mmff_get_counters(np.ctypeslib.ctypes.cast(cnt, np.ctypeslib.ctypes.c_void_p))
     lib.mmff_set_counting(0)
     w.restore()
@@ -475,7 +475,7 @@ def count_work(w, lib, nstep_max):
     GridFF samples, system force evaluations."""
     lib.mmff_set_counting(1)
     w.restore(); w.relax(nstep_max, FCONV, 1)
-    cnt = (np.ctypeslib.ctypes.c_ulonglong * 3)()
+    cnt = (np.ctypeslib.ctypes.c_ulonglong * 5)()
     lib.mmff_get_counters(np.ctypeslib.ctypes.cast(cnt, np.ctypeslib.ctypes.c_void_p))
     lib.mmff_set_counting(0)
     return int(cnt[0]), int(cnt[1]), int(cnt[2])

@@ -76,6 +76,10 @@ struct Params {
     float slv[9];                          // substrate lattice vectors a, b, c
     float sK, sR2damp;                     // -alphaMorse, Rdamp^2
     float sg0[3];                          // grid origin: world = local + gorg + sg0
+    // shifted-image pair lists of the CTA relax kernels (null: none): vstride
+    // 32-bit words per CTA, the first vcap of them list entries
+    uint32_t* vlist;
+    int vstride, vcap;
 };
 
 // Counter-based uniform random number in [-1, 1) for the Langevin force:
@@ -699,6 +703,10 @@ constexpr int kCompactMinThreads = 256;
 // (short candidate lists, ordered rows), and without the tile code there the
 // code of their central tiles stays as it is.
 constexpr int kImageTileMinThreads = 128;
+// shifted-image pair lists of the CTA relax kernels: shifted images handled
+// (2-D cells have 8) and the average list entries per atom a slot holds
+constexpr int kListMaxImages = 12;
+constexpr int kListEntriesPerAtom = 48;
 
 __host__ __device__ inline SmemLayout smem_layout_(int maxNA, int maxNN, int T, int nimg, bool compact) {
     SmemLayout L;

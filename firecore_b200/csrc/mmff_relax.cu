@@ -74,6 +74,17 @@ struct Engine {
     double e13 = 0.0;           // ENERGY: pair energies of the skipped 1-3 pairs (energy split)
     // pair-images evaluated by this thread (COUNT builds only)
     unsigned long long npair = 0;
+    // shifted-image pair lists of the current system (relax launches with
+    // P.vlist): entries (i | j << 12 | image << 24) in this CTA's slot of global
+    // scratch, then the positions at the last build.  Their state is
+    // block-uniform and sits in shared memory: [0] usable for this system (no
+    // overflow), [1] built and no atom moved more than half the skin since,
+    // [2] entries.
+    __device__ __forceinline__ uint32_t* vslot() const { return P.vlist + (size_t)blockIdx.x * P.vstride; }
+    __device__ __forceinline__ int* vstate() const {
+        __shared__ int st[3];
+        return st;
+    }
 
     __device__ Engine(const Params& p, const Systems& y, char* smem, const SmemLayout& l)
         : P(p), Y(y), L(l), sm(smem) {
@@ -102,6 +113,7 @@ struct Engine {
         xrow = Y.xmask + Y.moff[s];
         nbw = (natoms + 31) >> 5;
         pairbad = false;
+        if (tid == 0) { int* vs = vstate(); vs[0] = P.vlist != nullptr && natoms <= 4096; vs[1] = 0; vs[2] = 0; }
 #pragma unroll
         for (int k = 0; k < 9; k++) lv[k] = Y.lvec[9 * s + k];
         const float4 g = Y.gorg[s];
@@ -161,7 +173,9 @@ struct Engine {
     }
 
     // is image (ix,iy,iz) within the cutoff of the molecule's own box?
-    __device__ __forceinline__ bool image_active(int ix, int iy, int iz) const {
+    __device__ __forceinline__ bool image_active(int ix, int iy, int iz) const { return image_within(ix, iy, iz, P.Rc2); }
+    // ... within sqrt(R2) (the cutoff, or the cutoff plus the list skin)
+    __device__ __forceinline__ bool image_within(int ix, int iy, int iz, float R2) const {
         if (P.Rc2 <= 0.f) return true;
         if (ix == 0 && iy == 0 && iz == 0) return true;
         const float3 sh = image_shift(lv, ix, iy, iz);
@@ -169,15 +183,16 @@ struct Engine {
         const float gx = fmaxf(0.f, fabsf(sh.x) - (bbmax[0] - bbmin[0]));
         const float gy = fmaxf(0.f, fabsf(sh.y) - (bbmax[1] - bbmin[1]));
         const float gz = fmaxf(0.f, fabsf(sh.z) - (bbmax[2] - bbmin[2]));
-        return gx * gx + gy * gy + gz * gz < P.Rc2;
+        return gx * gx + gy * gy + gz * gz < R2;
     }
 
     // Candidate lists of the shifted images: atom j is a candidate of image
-    // (ix,iy,iz) when its shifted position lies within the cutoff of this
-    // system's own bounding box (no atom i can reach the others).  Lists are
+    // (ix,iy,iz) when its shifted position lies within sqrt(R2) (the cutoff,
+    // or the cutoff plus the list skin) of this system's own bounding box (no
+    // atom i can reach the others).  Lists are
     // ascending in j (ballot words, per-image prefix sums), so the pair sums
     // keep a fixed order.  All threads; contains barriers.
-    __device__ void build_candidates() {
+    __device__ void build_candidates(float R2) {
         const float4* spos = at<float4>(L.pos);
         uint32_t* words = at<uint32_t>(L.cwords);
         int* pref = at<int>(L.cpref);
@@ -194,13 +209,13 @@ struct Engine {
                     for (int ix = -npx; ix <= npx; ix++) {
                         if ((ix | iy | iz) == 0) continue;
                         bool c = false;
-                        if (j < natoms && image_active(ix, iy, iz)) {
+                        if (j < natoms && image_within(ix, iy, iz, R2)) {
                             const float3 sh = image_shift(lv, ix, iy, iz);
                             const float qx = p.x + sh.x, qy = p.y + sh.y, qz = p.z + sh.z;
                             const float gx = fmaxf(0.f, fmaxf(bbmin[0] - qx, qx - bbmax[0]));
                             const float gy = fmaxf(0.f, fmaxf(bbmin[1] - qy, qy - bbmax[1]));
                             const float gz = fmaxf(0.f, fmaxf(bbmin[2] - qz, qz - bbmax[2]));
-                            c = gx * gx + gy * gy + gz * gz < P.Rc2;
+                            c = gx * gx + gy * gy + gz * gz < R2;
                         }
                         const uint32_t bal = __ballot_sync(0xffffffffu, c);
                         if (lane == 0) words[k * nw + (base >> 5)] = bal;
@@ -507,6 +522,143 @@ struct Engine {
         if (j0 + lane < nJ) fix_add(facc + 3 * (int)Jl[j0 + lane], rj);
     }
 
+    // ---- shifted-image pair lists (Verlet lists with a skin) ------------------
+    // Of the pairs the candidate tiles of the shifted images evaluate, only a
+    // few percent lie inside the cutoff: for a large molecule the candidates
+    // of an image span its whole cross-section.  With lists, the ordered pairs
+    // (i, j + shift of image k) over every shifted image k closer than
+    // Rc + skin are collected once and evaluated every step (both orders of a
+    // pair are listed, so the force on i sums in registers and no reaction
+    // goes through the fixed-point atomics) until some atom has moved more
+    // than skin/2 since the build; then they are rebuilt.  The pairs inside
+    // the cutoff are the tiles' pairs, so forces differ from the tile path
+    // only in summation order.
+    static constexpr float kSkin = 1.0f;
+
+    // block-wide exclusive scan of one int per thread (total in every thread); tmp: nwarps ints
+    __device__ int block_scan(int x, int& total, int* tmp) {
+        int incl = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (lane == 31) tmp[warp] = incl;
+        __syncthreads();
+        int base = 0;
+        total = 0;
+        for (int w = 0; w < L.nwarps; w++) {
+            const int t = tmp[w];
+            if (w < warp) base += t;
+            total += t;
+        }
+        __syncthreads();
+        return base + incl - x;
+    }
+
+    // rebuild this system's lists from the current positions; false
+    // (block-uniform) when they do not fit in the slot.  All threads; barriers.
+    __device__ bool list_build(const float4* spos) {
+        const float Rv = sqrtf(P.Rc2) + kSkin, Rv2 = Rv * Rv;
+        build_candidates(Rv2);
+        const int* ccnt = at<int>(L.ccnt);
+        const unsigned short* clist = at<unsigned short>(L.clist);
+        uint32_t* ent = vslot();
+        // rows: (shifted image k, candidate i of its mirror), k-major; thread tid takes rows [r0, r1)
+        int R = 0;
+        for (int k = 0; k < L.nimg; k++) R += ccnt[L.nimg - 1 - k];
+        const int r0 = (int)((long long)R * tid / T), r1 = (int)((long long)R * (tid + 1) / T);
+        int* tmp = reinterpret_cast<int*>(at<long long>(L.facc));   // unused until the pair sums start
+        int off = 0, total = 0;
+        for (int pass = 0; pass < 2; pass++) {           // count, then write at the scanned offset
+            int c = 0, k = 0, base = 0;
+            for (int r = r0; r < r1; r++) {
+                while (r >= base + ccnt[L.nimg - 1 - k]) { base += ccnt[L.nimg - 1 - k]; k++; }
+                const int i = clist[(L.nimg - 1 - k) * L.maxNA + (r - base)];
+                const int nxi = 2 * P.npbc[0] + 1, nyi = 2 * P.npbc[1] + 1;
+                const int ipbc = k < L.nimg / 2 ? k : k + 1;      // image index with the central one
+                const float3 sh = image_shift(lv, ipbc % nxi - P.npbc[0], (ipbc / nxi) % nyi - P.npbc[1],
+                                              ipbc / (nxi * nyi) - P.npbc[2]);
+                const float4 pi = spos[i];
+                const float qx = pi.x - sh.x, qy = pi.y - sh.y, qz = pi.z - sh.z;
+                const unsigned short* Jl = clist + k * L.maxNA;
+                const int nJ = ccnt[k];
+                for (int jj = 0; jj < nJ; jj++) {
+                    const int j = Jl[jj];
+                    const float4 pj = spos[j];
+                    const float dx = pj.x - qx, dy = pj.y - qy, dz = pj.z - qz;
+                    if (!(fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < Rv2) || image_excluded(i, j, ipbc)) continue;
+                    if (pass == 1) ent[off + c] = (uint32_t)i | ((uint32_t)j << 12) | ((uint32_t)k << 24);
+                    c++;
+                }
+            }
+            if (pass == 0) {
+                off = block_scan(c, total, tmp);
+                if (total > P.vcap) return false;
+            }
+        }
+        float4* vp = reinterpret_cast<float4*>(ent + P.vcap);
+        for (int a = tid; a < natoms; a += T) vp[a] = spos[a];
+        if (tid == 0) vstate()[2] = total;
+        __syncthreads();
+        return true;
+    }
+
+    // excluded pair of the shifted image ipbc (NBFF::evalLJQs_ng4_PBC_atom,
+    // NBFF.h:590-607): i itself, and the bonded neighbours of i whose cell is this image
+    __device__ __forceinline__ bool image_excluded(int i, int j, int ipbc) {
+        if (j == i) return true;
+        const int4 ng = ngs(i), ngC = ngc(i);
+        return (ngC.x == ipbc && ng.x == j) || (ngC.y == ipbc && ng.y == j) || (ngC.z == ipbc && ng.z == j) ||
+               (ngC.w == ipbc && ng.w == j);
+    }
+
+    // the listed pairs of the shifted images into the fixed-point sums.  Each
+    // thread takes a contiguous run of entries (equal shares): consecutive
+    // entries mostly share atom i and image k, so the force on i adds up in
+    // registers and goes to the fixed-point sums once per run of i, the image
+    // shift is recomputed only when k changes, and the next entry's load
+    // overlaps the current pair.  Every pair is listed in both orders: half
+    // of its energy each time, no reaction.
+    template <bool HB>
+    __device__ void list_pairs(const float4* spos, const float4* sREQ, long long* facc, float& ec) {
+        const float Rc2 = P.Rc2, kq = P.kq_rc2, rc = sqrtf(1.f / kq);
+        const int nxi = 2 * P.npbc[0] + 1, nyi = 2 * P.npbc[1] + 1;
+        const uint32_t* ent = vslot();
+        const int n = vstate()[2];
+        const int q0 = (int)((long long)n * tid / T), q1 = (int)((long long)n * (tid + 1) / T);
+        if (q0 >= q1) return;
+        int ci = -1, ck = -1;
+        float3 sh = make_float3(0.f, 0.f, 0.f), fi = make_float3(0.f, 0.f, 0.f);
+        float4 pi = make_float4(0.f, 0.f, 0.f, 0.f), Ri = pi;
+        uint32_t wn = __ldcg(ent + q0);
+        for (int q = q0; q < q1; q++) {
+            const uint32_t w = wn;
+            if (q + 1 < q1) wn = __ldcg(ent + q + 1);
+            const int i = (int)(w & 0xFFFu), j = (int)((w >> 12) & 0xFFFu), k = (int)(w >> 24);
+            if (i != ci) {
+                if (ci >= 0) fix_add(facc + 3 * ci, fi);
+                ci = i; fi = make_float3(0.f, 0.f, 0.f);
+                pi = spos[i]; Ri = sREQ[i];
+            }
+            if (k != ck) {
+                ck = k;
+                const int ipbc = k < L.nimg / 2 ? k : k + 1;
+                sh = image_shift(lv, ipbc % nxi - P.npbc[0], (ipbc / nxi) % nyi - P.npbc[1], ipbc / (nxi * nyi) - P.npbc[2]);
+            }
+            const float4 pj = spos[j];
+            const float dx = pj.x + sh.x - pi.x, dy = pj.y + sh.y - pi.y, dz = pj.z + sh.z - pi.z;
+            bool ok;
+            float e = 0.f;
+            const float F = pair_force<ENERGY, HB>(dx, dy, dz, Ri, sREQ[j], false, Rc2, kq, rc, true, ok, e);
+            if (ENERGY) ec += 0.5f * e;
+            if (!ok) continue;
+            if (COUNT) npair++;
+            fi.x = fmaf(dx, F, fi.x); fi.y = fmaf(dy, F, fi.y); fi.z = fmaf(dz, F, fi.z);
+        }
+        fix_add(facc + 3 * ci, fi);
+    }
+
     // mirror pair (k, nimg-1-k): tiles (true) or ordered rows of both images.
     // Cost in pair evaluations: a tile evaluates 32 x 32 pairs at ~1.2 times
     // the cost of an ordered pair (the reaction and its rotation); the rows
@@ -705,8 +857,35 @@ struct Engine {
                 for (int iy = -npy; iy <= npy; iy++)
                     for (int ix = -npx; ix <= npx; ix++)
                         if ((ix | iy | iz) != 0) any_shift |= image_active(ix, iy, iz);
-            const bool lists = L.nimg > 0 && any_shift;
-            if (lists) build_candidates();
+            // pair lists of the shifted images (relax kernels with a scratch slot):
+            // kept while no atom moved more than skin/2 since their build
+            bool vrows = false;
+            int* vs = vstate();
+            if (vs[0] && any_shift && P.Rc2 > 0.f && L.nimg > 0 && L.nimg <= kListMaxImages) {
+                bool need = !vs[1];
+                if (!need) {
+                    const float4* vp = reinterpret_cast<const float4*>(vslot() + P.vcap);
+                    const float lim2 = 0.25f * kSkin * kSkin;
+                    int moved = 0;
+                    for (int a = tid; a < natoms; a += T) {
+                        const float4 p = spos[a], q = vp[a];
+                        const float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
+                        moved |= !(fmaf(dx, dx, fmaf(dy, dy, dz * dz)) <= lim2);
+                    }
+                    need = __syncthreads_or(moved) != 0;
+                }
+                if (need) {
+                    if (COUNT && tid == 0) atomicAdd(Y.counters + 3, 1ull);
+                    const bool built = list_build(spos);
+                    __syncthreads();                      // every thread has read the state
+                    if (tid == 0) { vs[0] = built; vs[1] = built; }
+                    __syncthreads();
+                }
+                vrows = vs[0] != 0;
+                if (COUNT && tid == 0 && vrows) atomicAdd(Y.counters + 4, (unsigned long long)vs[2]);
+            }
+            const bool lists = !vrows && L.nimg > 0 && any_shift;
+            if (lists) build_candidates(P.Rc2);
             const int central = (npz * nyi + npy) * nxi + npx;
             // central image and (with candidate lists) the shifted images:
             // every unordered pair once or ordered rows, into fixed-point sums
@@ -718,9 +897,11 @@ struct Engine {
                 if (hasH) {
                     if (lists) pair_tiles<true, true>(spos, sREQ, pbc, central, facc, ec);
                     else pair_tiles<true, false>(spos, sREQ, pbc, central, facc, ec);
+                    if (vrows) list_pairs<true>(spos, sREQ, facc, ec);
                 } else {
                     if (lists) pair_tiles<false, true>(spos, sREQ, pbc, central, facc, ec);
                     else pair_tiles<false, false>(spos, sREQ, pbc, central, facc, ec);
+                    if (vrows) list_pairs<false>(spos, sREQ, facc, ec);
                 }
                 if (ENERGY) Enb += (double)ec;
             }
@@ -730,7 +911,7 @@ struct Engine {
                                      (float)facc[3 * a + 2] * (1.f / kFix), 0.f);
             // without candidate lists: the other images of the bounding-box test,
             // ordered pairs (i, j + shift), S lanes per atom
-            if (!lists && any_shift) {
+            if (!lists && !vrows && any_shift) {
                 __syncthreads();
                 const int nunits = natoms * S;
                 for (int u0 = 0; u0 < nunits; u0 += T) {
@@ -952,6 +1133,8 @@ template <int T> constexpr int relax_min_blocks() {
     return T == 64 ? MMFF_MINB_T64 : T == 128 ? MMFF_MINB_T128 : T == 256 ? MMFF_MINB_T256 : 1;
 }
 
+// P.vlist (null: none): scratch for the shifted-image pair lists, P.vstride
+// 32-bit words per CTA (P.vcap entries, then 4 * maxNA words of positions)
 template <int T, int S, bool COUNT>
 __global__ void __launch_bounds__(T, relax_min_blocks<T>()) relax_kernel(Params P, Systems Y, const int* __restrict__ queue, int nqueue,
                                                   int* counter, int maxNA, int maxNN) {

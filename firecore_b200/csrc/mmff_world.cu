@@ -78,6 +78,10 @@ struct Bucket {
     DBuf<int> queue;
     int smem = 0, grid = 0;
     int cls = 0;                   // size class (see size_class)
+    // CTA relax kernels with a cutoff and a 2-D cell: scratch for the shifted-image
+    // pair lists, vstride 32-bit words per resident CTA (0: none)
+    DBuf<uint32_t> vl;
+    int vstride = 0;
 };
 
 // autotuned launch configuration of one size class (kind -1: heuristic)
@@ -113,6 +117,7 @@ struct World {
     // position springs (relax only)
     DBuf<float4> d_constr, d_constrK;
     bool has_constr = false;
+    bool pair_lists = true;        // shifted-image pair lists in the CTA relax kernels (mmff_set_pair_lists)
     // distance / angle constraints (mmff_set_bond_constraints)
     DBuf<int4> d_dci, d_aci;
     DBuf<float4> d_dca, d_dcb, d_aca;
@@ -293,6 +298,14 @@ int config_bucket(Bucket& B, int kind, int apl, int T, int S) {
     const int per_block = B.kind ? 4 : 1;
     const int nblk = ((int)B.sys.size() + per_block - 1) / per_block;
     B.grid = std::min(nblk, occ * nsm);
+    B.vstride = 0;
+    if (kind == 0 && W.Rcut > 0 && B.maxNA <= 4096) {
+        const int nimg = shifted_images(W.flags, W.npbc);
+        if (nimg > 0 && nimg <= kListMaxImages) {
+            B.vstride = B.maxNA * (kListEntriesPerAtom + 4);
+            if (B.vl.ensure((size_t)B.grid * B.vstride)) return -1;
+        }
+    }
     if (B.queue.ensure(B.sys.size())) return -1;
     CK(cudaMemcpy(B.queue.p, B.sys.data(), B.sys.size() * sizeof(int), cudaMemcpyHostToDevice));
     return 0;
@@ -397,7 +410,7 @@ int build_xmask() {
 }
 
 int build_buckets() {
-    for (auto& B : W.buckets) B.queue.release();
+    for (auto& B : W.buckets) { B.queue.release(); B.vl.release(); }
     W.buckets.clear();
     W.graph_valid = false;
     std::vector<std::vector<int>> groups(6);
@@ -444,6 +457,14 @@ struct PinnedBuf {
 PinnedBuf g_stage_a, g_stage_b;
 
 
+// the bucket's pair-list scratch into the launch parameters (CTA relax kernels)
+void set_lists(Params& P, const Bucket& B) {
+    const bool on = W.pair_lists && B.kind == 0 && B.vstride > 4 * B.maxNA && B.vl.p;
+    P.vlist = on ? B.vl.p : nullptr;
+    P.vstride = on ? B.vstride : 0;
+    P.vcap = on ? B.vstride - 4 * B.maxNA : 0;
+}
+
 // the launches of one relax call on the library stream: reset the work
 // counters, fork to one stream per bucket, one persistent kernel per bucket
 // (systems claimed through the bucket's queue), join
@@ -461,6 +482,7 @@ int enqueue_relax(const Params& P) {
         int nq = (int)B.sys.size();
         int* ctr = W.d_counter.p + b;
         int mna = B.maxNA, mnn = B.maxNN;
+        set_lists(Pc, B);
         void* args[] = {&Pc, &Y, &q, &nq, &ctr, &mna, &mnn};
         CK(cudaLaunchKernel(fn, dim3(B.grid), dim3(B.T), args, B.smem, st));
         if (!g_capturing) g_launches++;
@@ -785,6 +807,15 @@ int mmff_set_bond_constraints(int ndist, const int* dist_idx, const double* dist
     return 0;
 }
 
+// Shifted-image pair lists of the CTA relax kernels on (1, default) or off (0):
+// off evaluates the candidate tiles of the shifted images every step.
+int mmff_set_pair_lists(int on) {
+    if (ensure_ready()) return -1;
+    W.pair_lists = on != 0;
+    W.version++;
+    return 0;
+}
+
 // Restore positions, velocities and FIRE state from the copy kept at upload (device to device).
 int mmff_systems_restore(void) {
     if (ensure_ready()) return -1;
@@ -1000,6 +1031,7 @@ int mmff_autotune(int nstep_probe, int max_sample, float* report, int report_cap
                 const int* q = B.queue.p;
                 int nq = (int)B.sys.size(), mna = B.maxNA, mnn = B.maxNN;
                 int* ctr = W.d_counter.p + 32;
+                set_lists(P, B);
                 void* args[] = {&P, &Y, &q, &nq, &ctr, &mna, &mnn};
                 float ms = 0.f;
                 for (int rep = 0; rep < 2; rep++) {        // first launch warms caches and clocks
@@ -1018,6 +1050,7 @@ int mmff_autotune(int nstep_probe, int max_sample, float* report, int report_cap
                 cudaGetLastError();
             }
             B.queue.release();
+            B.vl.release();
             if (report && nrep < report_cap) {
                 const float row[6] = {(float)cls, (float)c.kind, (float)c.apl, (float)c.T, (float)c.S, us};
                 for (int j = 0; j < 6; j++) report[6 * nrep + j] = row[j];
@@ -1147,7 +1180,7 @@ int mmff_set_counting(int on) {
 }
 int mmff_get_counters(unsigned long long* out) {
     if (mmff_sync()) return -1;
-    CK(cudaMemcpy(out, W.d_stats.p, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(out, W.d_stats.p, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
     return 0;
 }
 

@@ -74,6 +74,11 @@ class World:
         """Per-atom GridFF stencil cache of the CTA relax kernels (bit-identical results)."""
         _check(self.lib.mmff_set_grid_cache(int(on)), "mmff_set_grid_cache")
 
+    def set_pair_lists(self, on: bool = True):
+        """Shifted-image pair lists in the CTA relax kernels (cutoff, 2-D cell):
+        on (default) or per-step candidate tiles."""
+        _check(self.lib.mmff_set_pair_lists(int(bool(on))), "mmff_set_pair_lists")
+
     def set_graph(self, on: bool = True):
         """Replay mmff_relax as one captured CUDA graph per parameter set."""
         _check(self.lib.mmff_set_graph(int(on)), "mmff_set_graph")

@@ -137,6 +137,13 @@ int mmff_set_bond_constraints(int ndist, const int* dist_idx, const double* dist
  * stencil cell changes; off (0) every step gathers.  Results are
  * bit-identical either way; 260 B of device memory per atom. */
 int mmff_set_grid_cache(int on);
+/* No counterpart in the reference.  Shifted-image pair lists in the CTA relax
+ * kernels (cutoff and a 2-D cell): the pairs (atom, image of atom) closer than
+ * Rcut + 1 A are collected once and evaluated every step until an atom has
+ * moved 0.5 A since; then they are rebuilt (Verlet lists with a 1 A skin).
+ * The pairs inside the cutoff are those of the per-step candidate tiles, so
+ * results differ only in summation order.  on (1, default) or off (0). */
+int mmff_set_pair_lists(int on);
 /* Restore positions, velocities and FIRE state saved at upload (device copy). */
 int mmff_systems_restore(void);
 /* Overwrite positions (and velocities; NULL = 0); reset_fire != 0 resets dt,
@@ -205,7 +212,8 @@ double mmff_timer_stop(void);                        /* ms since mmff_timer_star
 /* Counting mode (on != 0): the relax kernels also count pair-images inside
  * the cutoff, atom B-spline samples and force evaluations; counters reset. */
 int mmff_set_counting(int on);
-/* out[3] = (pair-images, atom grid samples, force evaluations) since the reset */
+/* out[5] = (pair-images, atom grid samples, force evaluations, shifted-image
+ * pair-list builds, listed pairs evaluated) since the reset */
 int mmff_get_counters(unsigned long long* out);
 /* Measured denominators: FP32 FFMA throughput [TFLOP/s] and L2-resident
  * float4 read bandwidth [GB/s] over an mbytes MiB buffer; < 0 on error. */

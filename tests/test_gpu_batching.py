@@ -113,3 +113,73 @@ def test_queue_retires_and_refills_mixed_sizes(world, golden):
     assert (st["nsteps"] > 0).all() and (st["nsteps"] <= 400).all()
     assert (st["nsteps"][st["status"] == 2] == 400).all()
     world.set_graph(False)
+
+
+def test_pair_lists_match_candidate_tiles(world, golden):
+    """Shifted-image pair lists (Verlet lists with a 1 A skin, CTA kernels)
+    against the per-step candidate tiles, on molecules of 150-400 atoms in a
+    22.56 A cell with a 10 A cutoff (images of every large molecule within
+    reach): the same pair-images inside the cutoff in a step (the counting
+    kernels count each within-cutoff pair-image); 60 steps of damped dynamics
+    without noise (no discrete decisions, atoms moving several A, so the lists
+    are rebuilt) that agree to rounding; deterministic FIRE relaxations.  (FIRE
+    trajectories of tiles and lists are not compared step for step: its
+    velocity reset on cos(v, f) < 0 turns rounding differences into
+    different paths.)"""
+    import ctypes
+    b = uneven(world, golden, n=48, seed=11, lo=150, hi=400)
+    a, n, v = b.offsets()
+
+    def run(on, nsteps, count):
+        world.set_pair_lists(on)
+        world.lib.mmff_set_counting(1 if count else 0)
+        world.restore(); world.relax(nsteps, 1e-4, conv_mode=1)
+        st = world.state()
+        c = np.zeros(5, np.uint64)
+        world.lib.mmff_get_counters(c.ctypes.data_as(ctypes.c_void_p))
+        return st, c
+
+    def dyn(on):
+        world.set_pair_lists(on)
+        world.restore()
+        world.set_md(dt=0.05, gamma=0.5, T=0.0, seed=1)
+        world.md(60)
+        return world.state()
+
+    try:
+        _, c_tiles = run(False, 1, True)
+        _, c_lists = run(True, 1, True)
+        p0 = world.state()["pos"]
+        m_tiles, m_lists = dyn(False), dyn(True)
+        t_lists, _ = run(True, 400, False)
+        t_again, _ = run(True, 400, False)
+    finally:
+        world.set_pair_lists(True)
+        world.lib.mmff_set_counting(0)
+    assert c_tiles[0] > 0 and c_tiles[0] == c_lists[0], (c_tiles, c_lists)
+    # the workload reaches into the images: within-cutoff pair-images of the
+    # shifted images at the start, a sizeable share of the count
+    nimg = 0
+    for s in range(b.nsys):
+        p = b.pos[v[s]:v[s] + b.natoms[s]]
+        for ix, iy in ((1, 0), (0, 1), (1, 1), (1, -1)):
+            q = p + ix * b.lvec[s][0] + iy * b.lvec[s][1]
+            nimg += 2 * int((((p[:, None] - q[None]) ** 2).sum(-1) < 100.0).sum())
+    assert nimg > 0.01 * float(c_tiles[0]), (nimg, c_tiles)
+    moved = np.abs(m_lists["pos"] - p0).max()
+    assert moved > 1.0, moved                                          # rebuilds happened
+    # systems larger than the cell start with atoms on top of their own images
+    # (forces of 1e6 eV/A and more, which the fixed-point pair sums clamp per
+    # contribution, so tiles and lists differ there by construction): compared
+    # are the others
+    fair = []
+    for s in range(b.nsys):
+        p = b.pos[v[s]:v[s] + b.natoms[s]]
+        dmin = min(np.sqrt((((p[:, None] - (p[None] + ix * b.lvec[s][0] + iy * b.lvec[s][1])) ** 2).sum(-1)).min())
+                   for ix, iy in ((1, 0), (0, 1), (1, 1), (1, -1)))
+        fair.append(dmin > 1.5)
+    assert sum(fair) >= 40, sum(fair)
+    d = max(np.abs(m_tiles["pos"][v[s]:v[s + 1]] - m_lists["pos"][v[s]:v[s + 1]]).max()
+            for s in range(b.nsys) if fair[s])
+    assert d < 1e-3, d
+    assert np.array_equal(t_lists["pos"], t_again["pos"])          # deterministic
