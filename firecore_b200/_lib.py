@@ -73,7 +73,7 @@ def _declare(lib):
         "mmff_grid_sample": [c_int, c_void, c_void, c_void],
         "mmff_systems_upload": [c_int] + [c_void] * 14, "mmff_systems_restore": [],
         "mmff_systems_set_state": [c_void, c_void, c_int], "mmff_eval": [c_int],
-        "mmff_set_constraints": [c_void, c_void], "mmff_set_bond_constraints": [c_int, c_void, c_void, c_int, c_void, c_void], "mmff_set_grid_cache": [c_int], "mmff_set_pair_lists": [c_int],
+        "mmff_set_constraints": [c_void, c_void], "mmff_set_bond_constraints": [c_int, c_void, c_void, c_int, c_void, c_void], "mmff_set_grid_cache": [c_int], "mmff_set_pair_lists": [c_int, c_double],
         "mmff_relax": [c_int, c_double, c_int], "mmff_get_forces": [c_void], "mmff_get_energies": [c_void],
         "mmff_get_state": [c_void] * 6, "mmff_timer_start": [], "mmff_num_buckets": [],
         "mmff_bucket_info": [c_int, c_void], "mmff_set_counting": [c_int], "mmff_get_counters": [c_void],

@@ -80,6 +80,7 @@ struct Params {
     // 32-bit words per CTA, the first vcap of them list entries
     uint32_t* vlist;
     int vstride, vcap;
+    float vskin;                           // list skin [A]
 };
 
 // Counter-based uniform random number in [-1, 1) for the Langevin force:

@@ -523,6 +523,7 @@ struct Engine {
     }
 
     // ---- shifted-image pair lists (Verlet lists with a skin) ------------------
+    // (skin P.vskin, 1 A by default.)
     // Of the pairs the candidate tiles of the shifted images evaluate, only a
     // few percent lie inside the cutoff: for a large molecule the candidates
     // of an image span its whole cross-section.  With lists, the ordered pairs
@@ -533,7 +534,6 @@ struct Engine {
     // than skin/2 since the build; then they are rebuilt.  The pairs inside
     // the cutoff are the tiles' pairs, so forces differ from the tile path
     // only in summation order.
-    static constexpr float kSkin = 1.0f;
 
     // block-wide exclusive scan of one int per thread (total in every thread); tmp: nwarps ints
     __device__ int block_scan(int x, int& total, int* tmp) {
@@ -559,7 +559,7 @@ struct Engine {
     // rebuild this system's lists from the current positions; false
     // (block-uniform) when they do not fit in the slot.  All threads; barriers.
     __device__ bool list_build(const float4* spos) {
-        const float Rv = sqrtf(P.Rc2) + kSkin, Rv2 = Rv * Rv;
+        const float Rv = sqrtf(P.Rc2) + P.vskin, Rv2 = Rv * Rv;
         build_candidates(Rv2);
         const int* ccnt = at<int>(L.ccnt);
         const unsigned short* clist = at<unsigned short>(L.clist);
@@ -865,7 +865,7 @@ struct Engine {
                 bool need = !vs[1];
                 if (!need) {
                     const float4* vp = reinterpret_cast<const float4*>(vslot() + P.vcap);
-                    const float lim2 = 0.25f * kSkin * kSkin;
+                    const float lim2 = 0.25f * P.vskin * P.vskin;
                     int moved = 0;
                     for (int a = tid; a < natoms; a += T) {
                         const float4 p = spos[a], q = vp[a];

@@ -118,6 +118,7 @@ struct World {
     DBuf<float4> d_constr, d_constrK;
     bool has_constr = false;
     bool pair_lists = true;        // shifted-image pair lists in the CTA relax kernels (mmff_set_pair_lists)
+    double list_skin = 1.0;        // their skin [A]
     // distance / angle constraints (mmff_set_bond_constraints)
     DBuf<int4> d_dci, d_aci;
     DBuf<float4> d_dca, d_dcb, d_aca;
@@ -463,6 +464,7 @@ void set_lists(Params& P, const Bucket& B) {
     P.vlist = on ? B.vl.p : nullptr;
     P.vstride = on ? B.vstride : 0;
     P.vcap = on ? B.vstride - 4 * B.maxNA : 0;
+    P.vskin = (float)W.list_skin;
 }
 
 // the launches of one relax call on the library stream: reset the work
@@ -809,8 +811,13 @@ int mmff_set_bond_constraints(int ndist, const int* dist_idx, const double* dist
 
 // Shifted-image pair lists of the CTA relax kernels on (1, default) or off (0):
 // off evaluates the candidate tiles of the shifted images every step.
-int mmff_set_pair_lists(int on) {
+// skin > 0 sets the list skin [A] (default 1).
+int mmff_set_pair_lists(int on, double skin) {
     if (ensure_ready()) return -1;
+    if (skin > 0) {
+        if (skin > 5.0) return fail("mmff_set_pair_lists: skin %g A out of range (0, 5]", skin);
+        W.list_skin = skin;
+    }
     W.pair_lists = on != 0;
     W.version++;
     return 0;

@@ -74,10 +74,10 @@ class World:
         """Per-atom GridFF stencil cache of the CTA relax kernels (bit-identical results)."""
         _check(self.lib.mmff_set_grid_cache(int(on)), "mmff_set_grid_cache")
 
-    def set_pair_lists(self, on: bool = True):
+    def set_pair_lists(self, on: bool = True, skin: float = 0.0):
         """Shifted-image pair lists in the CTA relax kernels (cutoff, 2-D cell):
-        on (default) or per-step candidate tiles."""
-        _check(self.lib.mmff_set_pair_lists(int(bool(on))), "mmff_set_pair_lists")
+        on (default) or per-step candidate tiles; skin > 0 sets their skin [A]."""
+        _check(self.lib.mmff_set_pair_lists(int(bool(on)), float(skin)), "mmff_set_pair_lists")
 
     def set_graph(self, on: bool = True):
         """Replay mmff_relax as one captured CUDA graph per parameter set."""

@@ -139,11 +139,12 @@ int mmff_set_bond_constraints(int ndist, const int* dist_idx, const double* dist
 int mmff_set_grid_cache(int on);
 /* No counterpart in the reference.  Shifted-image pair lists in the CTA relax
  * kernels (cutoff and a 2-D cell): the pairs (atom, image of atom) closer than
- * Rcut + 1 A are collected once and evaluated every step until an atom has
- * moved 0.5 A since; then they are rebuilt (Verlet lists with a 1 A skin).
- * The pairs inside the cutoff are those of the per-step candidate tiles, so
- * results differ only in summation order.  on (1, default) or off (0). */
-int mmff_set_pair_lists(int on);
+ * Rcut + skin are collected once and evaluated every step until an atom has
+ * moved skin/2 since; then they are rebuilt (Verlet lists).  The pairs inside
+ * the cutoff are those of the per-step candidate tiles, so results differ
+ * only in summation order.  on (1, default) or off (0); skin > 0 sets the
+ * skin [A] (default 1, at most 5), skin <= 0 keeps it. */
+int mmff_set_pair_lists(int on, double skin);
 /* Restore positions, velocities and FIRE state saved at upload (device copy). */
 int mmff_systems_restore(void);
 /* Overwrite positions (and velocities; NULL = 0); reset_fire != 0 resets dt,
