@@ -125,3 +125,22 @@ H -0.360  1.030  0.000
 H -0.360 -0.515  0.890
 H -0.360 -0.515 -0.890  0.2
 """
+
+
+def polyethylene(ncell=4, noise=0.0, seed=0):
+    """xyz text of an infinite zigzag C chain along x, 4 CH2 units per cell (the
+    chain bonds across the cell wall), in an "lvs" cell of 5.08 x 8 x 20 A."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    lines = []
+    for i in range(ncell):
+        x, z = 1.27 * i, 10.0 + (0.42 if i % 2 else 0.0)
+        lines.append(("C", x, 0.0, z, -0.1))
+        s = 1.0 if i % 2 else -1.0
+        lines.append(("H", x, 0.89, z + 0.52 * s, 0.05))
+        lines.append(("H", x, -0.89, z + 0.52 * s, 0.05))
+    out = [str(len(lines)), f"lvs {1.27 * ncell:.4f} 0 0   0 8 0   0 0 20"]
+    for e, x, y, z, q in lines:
+        d = rng.normal(0, noise, 3) if noise > 0 else np.zeros(3)
+        out.append(f"{e} {x + d[0]:.6f} {y + d[1]:.6f} {z + d[2]:.6f} {q}")
+    return "\n".join(out) + "\n"

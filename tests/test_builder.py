@@ -148,3 +148,38 @@ def test_batch_of_typed_molecule_evaluates_in_the_oracle(tmp_path):
     F, E = O.eval_forces(b, O.make_params(flags=O.DEFAULT_FLAGS))
     assert np.isfinite(F).all() and np.isfinite(E).all()
     np.testing.assert_array_equal(E[0], E[1])
+
+
+@pytest.mark.skipif(not os.path.isfile(os.path.join(RES, "AtomTypes.dat")), reason="FireCore tree not present")
+@pytest.mark.parametrize("mol", ["polydiacetylene.xyz", "polydiacetylene_OH.xyz", "polymer-2.xyz"])
+def test_oracle_matches_firecore_on_periodic_polymers(mol):
+    """Bonds across the cell wall (neighCell != central image): FireCore's
+    periodic polymers, typed by this builder, evaluated by the FP64 oracle and by
+    FireCore's own eval_atom / evalLJQs_ng4_PBC_atom_omp through the reference
+    harness agree to rounding."""
+    import ctypes
+    from firecore_b200 import topology as T
+    from oracle import oracle as O
+    O.build_oracle(with_ref=True)
+    if not O.ref_available():
+        pytest.skip("reference harness not built")
+    d = _build(os.path.join(RES, "xyz", mol), T.table_paths(RES))
+    assert d["pbc"] and (d["neighCell"][d["neighs"] >= 0] != 4).any()     # bonds into the next cells
+    b = T.to_batch(d)
+    na, nn = d["natoms"], d["nnode"]
+    ref = O.ref()
+    p = lambda a: ctypes.c_void_p(a.ctypes.data)  # noqa: E731
+    pos = np.ascontiguousarray(b.pos)
+    arr = [np.ascontiguousarray(x) for x in (b.neighs, b.neighCell, b.REQs)]
+    nar = [np.ascontiguousarray(x) for x in (b.apars, b.bLs, b.bKs, b.Ksp, b.Kpp)]
+    lv = np.ascontiguousarray(b.lvec[0].reshape(9)); npbc = np.array([1, 1, 0], np.int32)
+    gn = np.array([4, 4, 8], np.int32); gp0 = np.zeros(3); gst = np.ones(3); C = np.zeros(4 * 4 * 8 * 3)
+    bk = np.zeros((na, 4), np.int32); ng = np.zeros((na, 4), np.int32)
+    for fl in (O.DEFAULT_FLAGS & ~O.GRID, O.BONDS | O.ANGLES | O.PISIGMA | O.PIPI | O.PBC):
+        ref.ref_setup(na, nn, p(pos), p(arr[0]), p(arr[1]), p(arr[2]), *[p(x) for x in nar], p(lv), p(npbc), fl, 1.5,
+                      p(gn), p(gp0), p(gst), p(C), p(bk), p(ng))
+        f = np.zeros((na + nn, 3)); e = np.zeros(4)
+        ref.ref_eval(p(f), p(e))
+        Fo, Eo = O.eval_forces(b, O.make_params(flags=fl, npbc=(1, 1, 0)))
+        assert np.abs(Fo - f).max() <= 1e-12 * max(1.0, np.abs(f).max())
+        assert np.abs(Eo[0] - e).max() <= 1e-12 * max(1.0, np.abs(e).max())

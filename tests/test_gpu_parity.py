@@ -4,6 +4,8 @@ golden outputs.  Tolerances (FP32 forces, FP64 reductions):
   energies : |E_gpu - E_ref| <= ETOL * (|E_bonded| + |E_nb| + |E_grid|)
   relaxed  : final energy within 1e-5 eV/atom, RMSD <= 1e-3 A
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -388,3 +390,41 @@ def test_bond_constraints_vs_oracle(world, golden, threads):
     l_gpu = np.linalg.norm(st["pos"][v[3] + 2] - st["pos"][v[3] + 17])
     l_orc = np.linalg.norm(r["pos"][v[3] + 2] - r["pos"][v[3] + 17])
     assert abs(l_gpu - l_orc) < 1e-2
+
+
+def test_periodic_chain_vs_oracle(world, golden):
+    """Bonds across the cell wall on the GPU: an infinite CH2 chain typed by the
+    FireCore-format builder (this project's own small tables), 8 noisy copies:
+    forces and energies of one evaluation, then relaxed geometries, against
+    the FP64 oracle (itself pinned to FireCore on FireCore's periodic polymers,
+    test_builder.py)."""
+    from builder_tables import polyethylene, write_tables
+    from firecore_b200 import topology as T
+    import tempfile
+    tmp = tempfile.mkdtemp()
+    tables = write_tables(os.path.join(tmp, "t"))
+    parts = []
+    for k in range(8):
+        path = os.path.join(tmp, f"pe{k}.xyz")
+        with open(path, "w") as f:
+            f.write(polyethylene(noise=0.05, seed=k))
+        parts.append(T.to_batch(T.build_xyz(path, tables)))
+    b = S.SystemBatch(*[np.concatenate([getattr(p, f) for p in parts]) for f in S.SystemBatch.__dataclass_fields__])
+    assert (b.neighCell[b.neighs >= 0] != 4).any()
+    flags = DEFAULT_FLAGS & ~O.GRID
+    ferr, eerr = check_eval(world, b, None, None, flags, npbc=(1, 1, 0))
+    assert ferr.max() < FTOL, ferr
+    assert eerr.max() < ETOL, eerr
+    world.set_params(flags=flags, npbc=(1, 1, 0))
+    world.set_fire(FireParams(Flim=10.0))
+    world.upload(b)
+    pos0 = world.state()["pos"]
+    world.relax(4000, 1e-4, conv_mode=1)
+    st = world.state()
+    world.set_fire(FireParams())
+    P = O.make_params(None, flags=flags, npbc=(1, 1, 0))
+    r = O.relax(b, P, O.make_fire(Flim=10.0), None, niter=4000, Fconv=1e-4, conv_mode=1, pos=pos0)
+    assert (st["status"] == 1).all() and (r["converged"] == 1).all()
+    _, Eg = O.eval_forces(b, P, None, pos=st["pos"])
+    _, Ec = O.eval_forces(b, P, None, pos=r["pos"])
+    assert (np.abs(Eg[:, 3] - Ec[:, 3]) / b.natoms).max() <= 1e-5
