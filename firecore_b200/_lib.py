@@ -85,7 +85,8 @@ def _declare(lib):
         "mmff_mlp_set_projection": [c_int], "mmff_mlp_project": [c_void, c_void], "mmff_mlp_wait_test": [],
         "mmff_mlp_plan": [c_void], "mmff_mlp_layout": [c_void],
         "mmff_set_graph": [c_int], "mmff_set_md": [c_double, c_double, c_double, ctypes.c_ulonglong],
-        "mmff_md": [c_int], "mmff_surf_upload": [c_int, c_void, c_void, c_void, c_void, c_double], "mmff_autotune": [c_int, c_int, c_void, c_int],
+        "mmff_md": [c_int], "mmff_set_explore": [c_int, c_int, c_int], "mmff_explore": [c_int, c_double, c_int],
+        "mmff_get_explore": [c_void, c_void], "mmff_surf_upload": [c_int, c_void, c_void, c_void, c_void, c_double], "mmff_autotune": [c_int, c_int, c_void, c_int],
         "mmff_get_tuning": [c_int, c_void], "mmff_set_tuning": [c_int, c_int, c_int, c_int, c_int],
         "mmff_build_xyz": [ctypes.c_char_p] * 5 + [c_int, c_void, c_int] + [c_void] * 12,
     }

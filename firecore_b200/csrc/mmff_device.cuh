@@ -63,11 +63,14 @@ struct Params {
     double Fconv2;
     int conv_mode;       // 0: sum f^2 ; 1: max |f|^2
     int nstep_max;       // steps allowed in this call
-    // Langevin drive (md_mode 1) instead of FIRE: MMFFsp3_loc::move_atom_Langevin
+    // Langevin drive (md_mode 1) instead of FIRE: MMFFsp3_loc::move_atom_Langevin;
+    // md_mode 2: the exploring cycle of GOpt (Langevin for n_explore steps after
+    // every minimum found, or after n_relax FIRE steps without one)
     int md_mode;
     float md_dt, md_gamma, md_noise;   // noise = sqrt(2 kB T gamma / dt)
     unsigned long long md_seed;
     int md_step0;                      // step index of the call's first step (random stream)
+    int n_explore, n_relax;            // md_mode 2 (n_relax <= 0: no give-up)
     // direct substrate term (F_SURF): substrate atoms in world coordinates
     const float4* __restrict__ surf_pos;
     const float4* __restrict__ surf_REQ;   // (R0, sqrt(E0), Q sqrt(k_e), H)
@@ -96,6 +99,20 @@ __host__ __device__ inline float langevin_rand(unsigned long long seed, long lon
     const unsigned long long key =
         seed ^ mix64(((unsigned long long)(unsigned)step << 32) ^ ((unsigned long long)vec << 2) ^ (unsigned long long)comp);
     return (float)(mix64(key) >> 40) * (2.0f / 16777216.0f) - 1.0f;
+}
+
+// Exploring cycle of the global optimiser (md_mode 2), one call per step before
+// the forces: a FIRE phase longer than n_relax steps is given up
+// (MolWorld_sp3_multi.h:797-803), then GOpt::update (GOpt.h:46-56) counts the
+// step and ends an exploring phase once it reaches n_explore steps.
+// ph = 2 * (steps in the phase) + exploring; returns bit 0: this step explores
+// (Langevin instead of FIRE), bit 1: a FIRE phase was given up.
+__device__ __forceinline__ int explore_step(int& ph, int n_explore, int n_relax) {
+    int ev = 0;
+    if (!(ph & 1) && n_relax > 0 && (ph >> 1) > n_relax) { ph = 1; ev = 2; }
+    ph += 2;
+    if ((ph & 1) && (ph >> 1) >= n_explore) ph = 0;
+    return ev | (ph & 1);
 }
 
 struct Systems {
@@ -138,6 +155,10 @@ struct Systems {
     float* fconv;                       // convergence measure at exit (sqrt)
     double4* energy;                    // eval only: (bonded, non-bonded, grid, total)
     unsigned long long* counters;       // counting builds: pair-images, atom grid samples, force evaluations
+    // exploring cycle (md_mode 2): per system (exploring, steps in the phase,
+    // minima found, relax phases given up); per vector the last minimum found
+    int4* gopt;
+    float4* minpos;                     // local frame, like pos
 };
 
 __device__ __forceinline__ float3 f3(float4 a) { return make_float3(a.x, a.y, a.z); }

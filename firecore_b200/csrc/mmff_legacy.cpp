@@ -246,6 +246,8 @@ struct LegacyWorld {
     // Langevin dynamics instead of FIRE when both are > 0
     double T = 0.0, gamma = 0.0;
     bool md_set = false;          // Langevin parameters passed to the device world
+    // exploring cycle of init(nExplore, nRelax) (GOpt): run(iParalel = 2) drives it
+    int nExplore = 0, nRelax = 0;
     // host mirrors (pyBall/MMFF_multi.py:238-256 shapes)
     std::vector<float> atoms, aforces, avel, constr, REQs, MMpars, BLs, BKs, Ksp, Kpp, lvecs, ilvecs, pbcshifts;
     // spring constants of the constr anchors (MolWorld_sp3_multi::constrK): -1 = no
@@ -436,8 +438,10 @@ void setVerbosity(int verbosity_, int idebug_) { g_verbosity = verbosity_; (void
 void* init(int nSys, char* xyz_name, char* surf_name, char* smile_name, bool bMMFF, bool bEpairs, int* nPBC, int* grid_nPBC,
            double gridStep, char* sElementTypes, char* sAtomTypes, char* sBondTypes, char* sAngleTypes, double T, double gamma,
            int nExplore, int nRelax, double pos_kick, double vel_kick, int GridFF) {
-    (void)smile_name; (void)bMMFF; (void)nExplore; (void)nRelax; (void)pos_kick; (void)vel_kick;
+    // pos_kick / vel_kick feed GOpt::apply_kick, which the reference never calls
+    (void)smile_name; (void)bMMFF; (void)pos_kick; (void)vel_kick;
     L.T = T; L.gamma = gamma; L.md_set = false;
+    L.nExplore = nExplore; L.nRelax = nRelax;
     L.dist_i.clear(); L.dist_p.clear(); L.ang_i.clear(); L.ang_p.clear();
     {   // a new world: the cell of an earlier init (its substrate or xyz) does not carry over
         const double lv0[9] = {20, 0, 0, 0, 20, 0, 0, 0, 20};
@@ -550,9 +554,22 @@ void* init(int nSys, char* xyz_name, char* surf_name, char* smile_name, bool bMM
 // selects the reference's CPU (-1, 0, 1) or OpenCL (2, 3, 4) drivers there;
 // this library has only the device path, so every value runs it.
 int run(int nstepMax, double dt, double Fconv, int ialg, double* outE, double* outF, int iParalel) {
-    (void)dt; (void)ialg; (void)iParalel;
+    (void)dt; (void)ialg;
     if (!L.ready) { set_error("run: init() first"); return -1; }
-    if (mmff_relax(nstepMax, Fconv, 0)) { set_error(mmff_last_error()); return -1; }
+    if (iParalel == 2 && L.nExplore > 0) {
+        // run_ocl_opt with GOpt (MolWorld_sp3_multi.h:1694-1846, 770-833): every
+        // replica cycles between FIRE and nExplore Langevin steps (time step =
+        // the FIRE dt_max, as evalVF_new sets it, MolWorld_sp3_multi.h:756-760);
+        // after init every replica starts exploring (MolWorld_sp3_multi.h:278).
+        // The cycle's state lives on the device until the systems are uploaded again.
+        if (mmff_get_explore(nullptr, nullptr)) {
+            if (mmff_set_md(L.fire[0], L.gamma, L.T, 12345ull) || mmff_set_explore(L.nExplore, L.nRelax, 1)) {
+                set_error(mmff_last_error()); return -1;
+            }
+            L.md_set = true;
+        }
+        if (mmff_explore(nstepMax, Fconv, 0)) { set_error(mmff_last_error()); return -1; }
+    } else if (mmff_relax(nstepMax, Fconv, 0)) { set_error(mmff_last_error()); return -1; }
     std::vector<int> ns(L.nSys);
     std::vector<double> fc(L.nSys);
     if (mmff_get_state(nullptr, nullptr, nullptr, nullptr, ns.data(), fc.data())) return -1;

@@ -1097,6 +1097,12 @@ struct Engine {
         }
     }
 
+    // copy of the positions just moved (each thread its own vectors, as in move)
+    __device__ void snapshot() {
+        const float4* spos = at<float4>(L.pos);
+        for (int v = tid; v < nvecs; v += T) Y.minpos[voff + v] = spos[v];
+    }
+
     __device__ void store_state(int status, int steps, float fconv, double dt, double damping, int lastNeg, double total) {
         const float4* spos = at<float4>(L.pos);
         const float4* svel = at<float4>(L.vel);
@@ -1156,7 +1162,15 @@ __global__ void __launch_bounds__(T, relax_min_blocks<T>()) relax_kernel(Params 
         E.bbox_from_smem();
         int status = ST_MAXSTEPS, itr = 0;
         float meas = 0.f;
+        int ph = 0;                 // exploring cycle: 2 * (steps in the phase) + exploring
+        if (P.md_mode == 2) { const int4 g = Y.gopt[s]; ph = 2 * g.y + (g.x != 0); }
         for (itr = 0; itr < P.nstep_max; itr++) {
+            bool expl = false;
+            if (P.md_mode == 2) {
+                const int ev = explore_step(ph, P.n_explore, P.n_relax);
+                expl = ev & 1;
+                if ((ev & 2) && threadIdx.x == 0) Y.gopt[s].w++;
+            }
             double d0 = 0, d1 = 0, d2 = 0;
             E.forces(d0, d1, d2);
             __syncthreads();
@@ -1166,7 +1180,7 @@ __global__ void __launch_bounds__(T, relax_min_blocks<T>()) relax_kernel(Params 
             E.assemble(vf, vv, ff, fmax2, bad);
             E.reduce4(vf, vv, ff, fmax2, bad);
             if (bad) { status = ST_NAN; break; }
-            if (P.md_mode) {        // Langevin drive: fixed number of steps, no FIRE
+            if (P.md_mode == 1) {   // Langevin drive: fixed number of steps, no FIRE
                 float mn[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, mx[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
                 E.move_md(P.md_step0 + itr, mn, mx);
                 total += 1.0;
@@ -1190,17 +1204,26 @@ __global__ void __launch_bounds__(T, relax_min_blocks<T>()) relax_kernel(Params 
                 lastNeg++;
             }
             float mn[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, mx[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
-            E.move(dt, cv, P.fire_variant == 1 ? cf : renorm_vf * cf, mn, mx);
+            // the FIRE scalars above evolve in exploring steps too (MolWorld_sp3.h:2401-2424)
+            if (expl) E.move_md(P.md_step0 + itr, mn, mx);
+            else E.move(dt, cv, P.fire_variant == 1 ? cf : renorm_vf * cf, mn, mx);
             total += 1.0;
             const double m = (P.conv_mode == 0) ? ff : (double)fmax2;
             meas = (float)sqrt(m);
-            if (m < P.Fconv2) { status = ST_CONVERGED; itr++; E.bbox_reduce(mn, mx); break; }
+            if (m < P.Fconv2 && !expl) {
+                if (P.md_mode != 2) { status = ST_CONVERGED; itr++; E.bbox_reduce(mn, mx); break; }
+                // a minimum (MolWorld_sp3.h:2465-2473): keep it, start exploring
+                E.snapshot();
+                if (threadIdx.x == 0) Y.gopt[s].z++;
+                ph = 1;
+            }
             E.bbox_reduce(mn, mx);   // contains the end-of-step barrier
         }
         // converged at step itr-1 (reference returns the loop index at break)
         const int steps = (status == ST_CONVERGED) ? itr - 1 : itr;
         __syncthreads();
         E.store_state(status, steps, meas, dt, damping, lastNeg, total);
+        if (P.md_mode == 2 && threadIdx.x == 0) { Y.gopt[s].x = ph & 1; Y.gopt[s].y = ph >> 1; }
         if (COUNT) {
             // force evaluations done for this system: itr loop iterations
             if (threadIdx.x == 0) {

@@ -657,6 +657,11 @@ struct WarpEngine {
         __syncwarp();
     }
 
+    // copy of the positions just moved (move ends with __syncwarp)
+    __device__ void snapshot() {
+        for (int v = lane; v < NV; v += 32) Y.minpos[voff + v] = sp[v];
+    }
+
     __device__ void store(int status, int steps, float meas, double dt, double damping, int lastNeg, double total) {
         for (int v = lane; v < NV; v += 32) Y.pos[voff + v] = sp[v];
 #pragma unroll
@@ -699,7 +704,15 @@ __global__ void __launch_bounds__(128, MMFF_WARP_MINB) relax_warp_kernel(Params 
         int lastNeg = (int)fs.z;
         int status = ST_MAXSTEPS, itr = 0;
         float meas = 0.f;
+        int ph = 0;                 // exploring cycle: 2 * (steps in the phase) + exploring
+        if (P.md_mode == 2) { const int4 g = Y.gopt[s]; ph = 2 * g.y + (g.x != 0); }
         for (itr = 0; itr < P.nstep_max; itr++) {
+            bool expl = false;
+            if (P.md_mode == 2) {
+                const int ev = explore_step(ph, P.n_explore, P.n_relax);
+                expl = ev & 1;
+                if ((ev & 2) && lane == 0) Y.gopt[s].w++;
+            }
             double d0 = 0, d1 = 0, d2 = 0;
             E.forces(d0, d1, d2);
             double vf, vv, ff;
@@ -707,7 +720,7 @@ __global__ void __launch_bounds__(128, MMFF_WARP_MINB) relax_warp_kernel(Params 
             bool bad;
             E.fire_sums(vf, vv, ff, fmax2, bad);
             if (bad) { status = ST_NAN; break; }
-            if (P.md_mode) {        // Langevin drive: fixed number of steps, no FIRE
+            if (P.md_mode == 1) {   // Langevin drive: fixed number of steps, no FIRE
                 E.move_md(P.md_step0 + itr);
                 total += 1.0;
                 meas = sqrtf(fmax2);
@@ -728,14 +741,23 @@ __global__ void __launch_bounds__(128, MMFF_WARP_MINB) relax_warp_kernel(Params 
                 if (lastNeg > P.minLastNeg) { dt = fmin(dt * P.finc, P.dt_max); damping = damping * P.falpha; }
                 lastNeg++;
             }
-            E.move(dt, cv, P.fire_variant == 1 ? cf : renorm_vf * cf);
+            // the FIRE scalars above evolve in exploring steps too (MolWorld_sp3.h:2401-2424)
+            if (expl) E.move_md(P.md_step0 + itr);
+            else E.move(dt, cv, P.fire_variant == 1 ? cf : renorm_vf * cf);
             total += 1.0;
             const double m = (P.conv_mode == 0) ? ff : (double)fmax2;
             meas = (float)sqrt(m);
-            if (m < P.Fconv2) { status = ST_CONVERGED; itr++; break; }
+            if (m < P.Fconv2 && !expl) {
+                if (P.md_mode != 2) { status = ST_CONVERGED; itr++; break; }
+                // a minimum (MolWorld_sp3.h:2465-2473): keep it, start exploring
+                E.snapshot();
+                if (lane == 0) Y.gopt[s].z++;
+                ph = 1;
+            }
         }
         const int steps = (status == ST_CONVERGED) ? itr - 1 : itr;
         E.store(status, steps, meas, dt, damping, lastNeg, total);
+        if (P.md_mode == 2 && lane == 0) { Y.gopt[s].x = ph & 1; Y.gopt[s].y = ph >> 1; }
         if (COUNT && lane == 0) {
             atomicAdd(Y.counters + 1, (unsigned long long)itr * (unsigned long long)E.N);
             atomicAdd(Y.counters + 2, (unsigned long long)itr);

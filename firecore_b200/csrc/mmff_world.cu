@@ -158,6 +158,10 @@ struct World {
     double md_dt = 0.05, md_gamma = 0.1, md_T = 300.0;
     unsigned long long md_seed = 12345;
     int md_step = 0;
+    // exploring cycle (mmff_set_explore; n_explore < 0: not set up for the current systems)
+    DBuf<int4> d_gopt;
+    DBuf<float4> d_minpos;
+    int n_explore = -1, n_relax = 0;
 };
 
 World W;
@@ -231,6 +235,7 @@ Systems make_systems() {
     Y.pos = W.d_pos.p; Y.vel = W.d_vel.p; Y.force = W.d_force.p; Y.fire = W.d_fire.p;
     Y.status = W.d_status.p; Y.nsteps = W.d_nsteps.p; Y.fconv = W.d_fconv.p; Y.energy = W.d_energy.p;
     Y.counters = W.d_stats.p;
+    Y.gopt = W.d_gopt.p; Y.minpos = W.d_minpos.p;
     return Y;
 }
 
@@ -723,6 +728,7 @@ int mmff_systems_upload(int nsys, const int* natoms, const int* nnode, const dou
     W.h_ng = std::move(hng); W.h_ngC = std::move(hngC); W.h_a13 = std::move(ha13);
     W.has_constr = false;           // springs belong to the systems they were set for
     W.ndcon = 0; W.nacon = 0;       // and so do the distance / angle constraints
+    W.n_explore = -1;               // and the state of the exploring cycle
     if (W.d_force.ensure(NV) || W.d_energy.ensure(nsys) || W.d_status.ensure(nsys) || W.d_nsteps.ensure(nsys) ||
         W.d_fconv.ensure(nsys) || W.d_counter.ensure(64) || W.d_stats.ensure(8) || W.d_gkey.ensure(NA) ||
         W.d_gcs.ensure((size_t)NA * 16) || clear_grid_cache())
@@ -963,6 +969,80 @@ int mmff_md(int nsteps) {
     P.md_step0 = W.md_step;
     if (enqueue_relax(P)) return -1;
     W.md_step += nsteps;
+    return 0;
+}
+
+// Exploring cycle of the global optimiser (GOpt.h:25-60 with
+// MolWorld_sp3_multi.h:770-833 and MolWorld_sp3.h:2290-2296,2397-2473): every
+// system relaxes with FIRE; a minimum (convergence measure below Fconv) is
+// kept and starts an exploring phase of Langevin steps (mmff_set_md's dt,
+// gamma, T and random stream); a FIRE phase longer than n_relax steps
+// (n_relax <= 0: never) is given up and starts one too; an exploring phase
+// ends after n_explore steps.  Resets the cycle's per-system state: exploring
+// (start_exploring != 0) or relaxing, no minima found yet, the kept minimum =
+// the current positions.  Uploading systems clears it.
+int mmff_set_explore(int n_explore, int n_relax, int start_exploring) {
+    if (ensure_ready()) return -1;
+    if (!W.nsys) return fail("no systems uploaded");
+    if (n_explore < 0) return fail("mmff_set_explore: n_explore must be >= 0");
+    if (W.d_gopt.ensure(W.nsys) || W.d_minpos.ensure(W.NV)) return -1;
+    std::vector<int4> h(W.nsys, make_int4(start_exploring ? 1 : 0, 0, 0, 0));
+    if (upload(W.d_gopt, h)) return -1;
+    CK(cudaMemcpyAsync(W.d_minpos.p, W.d_pos.p, W.NV * sizeof(float4), cudaMemcpyDeviceToDevice, W.stream));
+    CK(cudaStreamSynchronize(W.stream));
+    W.n_explore = n_explore;
+    W.n_relax = n_relax;
+    return 0;
+}
+
+// nsteps steps of the exploring cycle for every system (same persistent
+// kernels as relax; no system retires, so every system runs nsteps steps;
+// convergence measure as mmff_relax's conv_mode).  Asynchronous.
+int mmff_explore(int nsteps, double Fconv, int conv_mode) {
+    if (ensure_ready()) return -1;
+    if (!W.nsys) return fail("no systems uploaded");
+    if (W.n_explore < 0) return fail("mmff_explore: call mmff_set_explore for the current systems first");
+    if (nsteps < 0) return fail("mmff_explore: nsteps must be >= 0");
+    if (W.buckets_dirty && build_buckets()) return -1;
+    Params P = make_params(false, nsteps, Fconv, conv_mode);
+    const double kB = 8.617333262e-5;     // eV/K (const_kB)
+    P.md_mode = 2;
+    P.md_dt = (float)W.md_dt;
+    P.md_gamma = (float)W.md_gamma;
+    P.md_noise = (float)sqrt(2.0 * kB * W.md_T * W.md_gamma / W.md_dt);
+    P.md_seed = W.md_seed;
+    P.md_step0 = W.md_step;
+    P.n_explore = W.n_explore;
+    P.n_relax = W.n_relax;
+    if (enqueue_relax(P)) return -1;
+    W.md_step += nsteps;
+    return 0;
+}
+
+// State of the exploring cycle: gopt [nsys][4] = (exploring, steps in the
+// current phase, minima found, relax phases given up); minpos (nullable)
+// [sum(natoms+nnode)][3] = the last minimum found per system, in world
+// coordinates like mmff_get_state's positions (the positions of
+// mmff_set_explore's call where none was found yet).
+int mmff_get_explore(int* gopt, double* minpos) {
+    if (mmff_sync()) return -1;
+    if (W.n_explore < 0) return fail("mmff_get_explore: no exploring cycle set up for the current systems");
+    if (gopt) CK(cudaMemcpy(gopt, W.d_gopt.p, W.nsys * sizeof(int4), cudaMemcpyDeviceToHost));
+    if (minpos) {
+        std::vector<float4> h(W.NV);
+        CK(cudaMemcpy(h.data(), W.d_minpos.p, W.NV * sizeof(float4), cudaMemcpyDeviceToHost));
+        for (int s = 0; s < W.nsys; s++) {
+            const int v0 = W.desc[s].z, na = W.natoms[s], nn = W.nnode[s];
+            const double* c = W.orig.data() + 3 * s;
+            for (int i = 0; i < na + nn; i++) {
+                const float4 p = h[v0 + i];
+                const double sh = i < na ? 1.0 : 0.0;
+                minpos[3 * (v0 + i)] = sh * c[0] + p.x;
+                minpos[3 * (v0 + i) + 1] = sh * c[1] + p.y;
+                minpos[3 * (v0 + i) + 2] = sh * c[2] + p.z;
+            }
+        }
+    }
     return 0;
 }
 

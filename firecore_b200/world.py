@@ -230,6 +230,28 @@ class World:
         if sync:
             self.sync()
 
+    def set_explore(self, n_explore: int, n_relax: int = 0, start_exploring: bool = False):
+        """Set up (and reset) the exploring cycle of the global optimiser for the
+        current systems: n_explore Langevin steps (``set_md``'s drive) after every
+        minimum found or after n_relax FIRE steps without one (0: never)."""
+        _check(self.lib.mmff_set_explore(int(n_explore), int(n_relax), int(bool(start_exploring))),
+               "mmff_set_explore")
+
+    def explore(self, nsteps: int, Fconv: float = 1e-4, conv_mode: int = 1, sync: bool = True):
+        """nsteps steps of the exploring cycle for every system."""
+        _check(self.lib.mmff_explore(int(nsteps), float(Fconv), int(conv_mode)), "mmff_explore")
+        if sync:
+            self.sync()
+
+    def explore_state(self):
+        """(gopt [nsys, 4] = (exploring, steps in phase, minima found, phases given
+        up), the last minimum found [sum nvecs, 3] in world coordinates)."""
+        b = self.batch
+        gopt = np.zeros((b.nsys, 4), dtype=np.int32)
+        minpos = np.zeros((int(b.nvecs.sum()), 3))
+        _check(self.lib.mmff_get_explore(_lib.ptr(gopt), _lib.ptr(minpos)), "mmff_get_explore")
+        return gopt, minpos
+
     def sync(self):
         _check(self.lib.mmff_sync(), "mmff_sync")
 

@@ -184,6 +184,28 @@ int mmff_set_md(double dt, double gamma, double T, unsigned long long seed);
 int mmff_surf_upload(int nsub, const double* spos, const double* sREQ, const double* lvec, const int* nPBC,
                      double Rdamp);
 int mmff_md(int nsteps);
+/* Exploring cycle of the global optimiser (replaces GOpt, GOpt.h:25-60, as
+ * MolWorld_sp3_multi::updateMultiExploring, MolWorld_sp3_multi.h:770-833, and
+ * MolWorld_sp3::run_no_omp with bGopt, MolWorld_sp3.h:2290-2296,2397-2473,
+ * drive it; the reference steps it on the host every 10 GPU steps, here it
+ * runs per step inside the relax kernels).  Per system and step: a FIRE phase
+ * longer than n_relax steps (n_relax <= 0: never) is given up and an exploring
+ * phase starts; the step count of the phase advances and an exploring phase
+ * ends once it reaches n_explore; forces; the FIRE scalars update; the atoms
+ * move by the Langevin drive of mmff_set_md (exploring) or by FIRE; a relaxing
+ * system whose convergence measure drops below Fconv has found a minimum: the
+ * positions are kept, the count rises and an exploring phase starts.  No
+ * system retires: mmff_explore runs nsteps steps for every system.
+ * mmff_set_explore resets the state (start_exploring != 0: every system
+ * starts in an exploring phase, as MolWorld_sp3_multi does after init with
+ * bGopt); mmff_get_explore reads it back: gopt [nsys][4] = (exploring, steps
+ * in the phase, minima found, phases given up), minpos (nullable)
+ * [sum(natoms+nnode)][3] = the last minimum found, world coordinates (the
+ * positions at mmff_set_explore where none was found).  The reference's
+ * database of distinct minima and its group drives are not part of it. */
+int mmff_set_explore(int n_explore, int n_relax, int start_exploring);
+int mmff_explore(int nsteps, double Fconv, int conv_mode);
+int mmff_get_explore(int* gopt, double* minpos);
 /* Autotuner (no counterpart in the reference, which uses one fixed work-group
  * size): for each size class present (0: <= 32 atoms, 1: <= 64, 3: <= 128,
  * 4: <= 256, 5: larger), time every candidate launch configuration (warp per
@@ -285,9 +307,15 @@ void* init(int nSys, char* xyz_name, char* surf_name, char* smile_name, bool bMM
  * directory (the reference ignores the four file arguments, MMFFmulti_lib.cpp:85);
  * when those are absent the four names given are used, and when neither set
  * exists this library's own parameter table (a documented deviation).  Typing
- * with tables = mmff_build_xyz.  smile_name, nExplore, nRelax, pos_kick and
- * vel_kick are not used. */
+ * with tables = mmff_build_xyz.  T, gamma, nExplore and nRelax set up the
+ * exploring cycle of run(iParalel = 2); smile_name is not used, nor are
+ * pos_kick and vel_kick (the reference's GOpt::apply_kick is never called). */
 int   run(int nstepMax, double dt, double Fconv, int ialg, double* outE, double* outF, int iParalel);   /* :116 */
+/* run: FIRE relaxation of every replica for up to nstepMax steps (every
+ * iParalel); with iParalel = 2 and init's nExplore > 0, nstepMax steps of the
+ * exploring cycle instead (mmff_explore; Langevin time step = the FIRE dt_max,
+ * T and gamma from init, every replica starting in an exploring phase), as
+ * run_ocl_opt with GOpt does.  dt and ialg are ignored, as by the reference. */
 void  MDloop(int perframe, double Ftol, int iParalel, int perVF);           /* :134 */
 void  set_opt(double dt_max, double dt_min, double damp_max, double finc, double fdec, double falpha, int minLastNeg,
               double cvf_min, double cvf_max);                              /* :141 */

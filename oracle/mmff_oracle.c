@@ -781,6 +781,121 @@ void orc_md(int nsys, const int* natoms, const int* nnode, double* pos, double* 
     free_offsets(o);
 }
 
+/* ---------------- exploring cycle (GOpt) ---------------- */
+
+/* GOpt (GOpt.h:25-60) driven per step as MolWorld_sp3::run_no_omp does with
+ * bGopt (MolWorld_sp3.h:2290-2296 update at the top of the step, :2397-2424
+ * FIRE scalars and the Langevin / FIRE move, :2465-2473 a minimum starts
+ * exploring) plus the give-up branch of MolWorld_sp3_multi::updateMultiExploring
+ * (MolWorld_sp3_multi.h:797-803: a relax phase longer than nRelax steps starts
+ * exploring).  Per step: give-up check; step count + 1 and the end of an
+ * exploring phase at n_explore; forces (clamped by F->Flim); FIRE_update_params
+ * always; exploring: the Langevin move of orc_md (md_dt, gamma, T, stream
+ * (seed, vector, step0 + step)), else move_atom_FIRE; a relaxing system below
+ * Fconv has found a minimum: minpos <- positions, count + 1, exploring starts.
+ * gopt[s*4] = (exploring, steps in phase, minima found, phases given up), in
+ * and out; fire_state as orc_relax. */
+void orc_explore(int nsys, const int* natoms, const int* nnode,
+                 double* pos, double* vel, double* fire_state, int* gopt, double* minpos,
+                 const int* neighs, const int* neighCell, const int* bkneighs,
+                 const double* REQs, const double* apars, const double* bLs,
+                 const double* bKs, const double* Ksp, const double* Kpp,
+                 const double* lvec, const double* gridC, const ORC_params* P,
+                 const ORC_fire* F, int nsteps, double Fconv, int conv_mode,
+                 int n_explore, int n_relax, double md_dt, double gamma, double T,
+                 unsigned long long seed, int step0, int nthreads) {
+    offsets_t o = make_offsets(nsys, natoms, nnode);
+    size_t nvtot = (size_t)o.voff[nsys];
+    double* force = (double*)calloc(nvtot * 3 + 3, sizeof(double));
+    const double kB = 8.617333262e-5;
+    const double noise = sqrt(2.0 * kB * T * gamma / md_dt);
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 1)
+#endif
+    for (int s = 0; s < nsys; s++) {
+        sysview S;
+        setup_view(&S, s, &o, natoms, nnode, pos, force, neighs, neighCell, bkneighs, REQs,
+                   apars, bLs, bKs, Ksp, Kpp, lvec, P);
+        double* p = pos + 3 * o.voff[s];
+        double* v = vel + 3 * o.voff[s];
+        double* fst = fire_state + 4 * s;
+        int* g = gopt + 4 * s;
+        double dt = fst[0], damping = fst[1];
+        int lastNeg = (int)fst[2];
+        double Ep[4] = {0, 0, 0, 0};
+        const int nv = S.nvecs;
+        for (int it = 0; it < nsteps; it++) {
+            if (!g[0] && n_relax > 0 && g[1] > n_relax) { g[3]++; g[0] = 1; g[1] = 0; }
+            g[1]++;
+            if (g[0] && g[1] >= n_explore) { g[0] = 0; g[1] = 0; }
+            const int expl = g[0];
+            eval_system(&S, P, gridC, Ep);
+            double vf = 0, vv = 0, ff = 0, fmax2 = 0;
+            for (int i = 0; i < nv; i++) {
+                double* fi = S.force + 3 * i;
+                double f2 = fi[0] * fi[0] + fi[1] * fi[1] + fi[2] * fi[2];
+                if (F->Flim > 0 && f2 > F->Flim * F->Flim) {
+                    double c = F->Flim / sqrt(f2); fi[0] *= c; fi[1] *= c; fi[2] *= c;
+                    f2 = fi[0] * fi[0] + fi[1] * fi[1] + fi[2] * fi[2];
+                }
+                for (int k = 0; k < 3; k++) { vf += v[3 * i + k] * fi[k]; vv += v[3 * i + k] * v[3 * i + k]; ff += fi[k] * fi[k]; }
+                if (f2 > fmax2 || f2 != f2) fmax2 = f2;
+            }
+            double f_len = sqrt(ff), v_len = sqrt(vv);
+            double cos_vf = vf / (f_len * v_len + 1e-32);
+            double renorm_vf = v_len / (f_len + 1e-32);
+            double cv, cf;
+            if (cos_vf < 0.0) { cv = F->cv_kill; cf = 0.; } else { cv = 1 - damping; cf = damping; }
+            cf = renorm_vf * cf;
+            if (cos_vf < 0.0) {
+                dt = fmax(dt * F->fdec, F->dt_min);
+                lastNeg = 0;
+                damping = F->damp_max;
+            } else {
+                if (lastNeg > F->minLastNeg) { dt = fmin(dt * F->finc, F->dt_max); damping = damping * F->falpha; }
+                lastNeg++;
+            }
+            const double dtf = (double)(float)dt;
+            const double cfm = (F->variant == 1) ? cf : renorm_vf * cf;
+            for (int i = 0; i < nv; i++) {
+                v3 f = ld3(S.force + 3 * i), vi = ld3(v + 3 * i), pi = ld3(p + 3 * i);
+                const int bPi = i >= S.natoms;
+                if (bPi) f = vaddmul(f, pi, -vdot(pi, f));
+                if (expl) {
+                    f = vaddmul(f, vi, -gamma);
+                    const long long gv = (long long)o.voff[s] + i;
+                    v3 r = {orc_langevin_rand(seed, gv, step0 + it, 0), orc_langevin_rand(seed, gv, step0 + it, 1),
+                            orc_langevin_rand(seed, gv, step0 + it, 2)};
+                    f = vaddmul(f, r, noise);
+                    vi = vaddmul(vi, f, md_dt);
+                    if (bPi) vi = vaddmul(vi, pi, -vdot(pi, vi));
+                    pi = vaddmul(pi, vi, md_dt);
+                } else {
+                    vi = vmul(vi, cv);
+                    vi = vaddmul(vi, f, dtf + cfm);
+                    if (bPi) vi = vaddmul(vi, pi, -vdot(pi, vi));
+                    pi = vaddmul(pi, vi, dtf);
+                }
+                if (bPi) {
+                    double l = sqrt(pi.x * pi.x + pi.y * pi.y + pi.z * pi.z);
+                    pi = vmul(pi, 1.0 / l);
+                }
+                st3(p + 3 * i, pi); st3(v + 3 * i, vi);
+            }
+            const double meas = (conv_mode == 0) ? ff : fmax2;
+            if (!expl && meas < Fconv * Fconv) {
+                memcpy(minpos + 3 * o.voff[s], p, sizeof(double) * 3 * (size_t)nv);
+                g[2]++; g[0] = 1; g[1] = 0;
+            }
+        }
+        fst[0] = dt; fst[1] = damping; fst[2] = (double)lastNeg;
+        free_view(&S);
+    }
+    free(force);
+    free_offsets(o);
+}
+
 /* ---------------- grid construction (GridFF.h:582-635, 847-891) ---------------- */
 
 void orc_grid_potentials(int nsub, const double* spos, const double* sREQ,

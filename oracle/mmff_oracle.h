@@ -117,6 +117,18 @@ void orc_md(int nsys, const int* natoms, const int* nnode, double* pos, double* 
             const double* lvec, const double* gridC, const ORC_params* P,
             int nsteps, double dt, double gamma, double T, unsigned long long seed, int step0,
             double Flim, int nthreads);
+/* Exploring cycle of GOpt on top of FIRE and the Langevin drive (see the
+ * definition for the step order); gopt[s*4] = (exploring, steps in phase,
+ * minima found, phases given up), minpos [nvecs*3] = last minimum found. */
+void orc_explore(int nsys, const int* natoms, const int* nnode,
+                 double* pos, double* vel, double* fire_state, int* gopt, double* minpos,
+                 const int* neighs, const int* neighCell, const int* bkneighs,
+                 const double* REQs, const double* apars, const double* bLs,
+                 const double* bKs, const double* Ksp, const double* Kpp,
+                 const double* lvec, const double* gridC, const ORC_params* P,
+                 const ORC_fire* F, int nsteps, double Fconv, int conv_mode,
+                 int n_explore, int n_relax, double md_dt, double gamma, double T,
+                 unsigned long long seed, int step0, int nthreads);
 /* the uniform random numbers of orc_md (SplitMix64 of seed, vector, step, component) */
 double orc_langevin_rand(unsigned long long seed, long long vec, int step, int comp);
 

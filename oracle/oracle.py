@@ -196,6 +196,33 @@ def md(b, P: ORCParams, gridC=None, nsteps=10, dt=0.05, gamma=0.1, T=300.0, seed
     return dict(pos=pos, vel=vel)
 
 
+def explore(b, P: ORCParams, F: ORCFire, gridC=None, nsteps=10, Fconv=1e-4, conv_mode=1, n_explore=10, n_relax=0,
+            dt=0.05, gamma=0.1, T=300.0, seed=12345, step0=0, pos=None, vel=None, fire_state=None, gopt=None,
+            minpos=None, nthreads=0):
+    """Exploring cycle of GOpt (orc_explore): FIRE relaxation, a Langevin phase of
+    n_explore steps after every minimum found or after n_relax FIRE steps without
+    one. Returns dict(pos, vel, fire_state, gopt [nsys, 4], minpos)."""
+    lib = orc()
+    pos = np.array(b.pos if pos is None else pos, np.float64, order="C")
+    vel = np.zeros_like(pos) if vel is None else np.array(vel, np.float64, order="C")
+    if fire_state is None:
+        fire_state = np.zeros((b.nsys, 4))
+        fire_state[:, 0] = F.dt_max
+        fire_state[:, 1] = F.damp_max
+    fire_state = np.array(fire_state, np.float64, order="C")
+    gopt = np.zeros((b.nsys, 4), np.int32) if gopt is None else np.array(gopt, np.int32, order="C")
+    minpos = pos.copy() if minpos is None else np.array(minpos, np.float64, order="C")
+    keep = [np.ascontiguousarray(b.natoms, np.int32), np.ascontiguousarray(b.nnode, np.int32)]
+    g = None if gridC is None else np.ascontiguousarray(gridC, np.float64)
+    arrs = _sysarrays(b)
+    lib.orc_explore(ctypes.c_int(b.nsys), _p(keep[0]), _p(keep[1]), _p(pos), _p(vel), _p(fire_state), _p(gopt),
+                    _p(minpos), *[_p(a) for a in arrs], _p(g), ctypes.byref(P), ctypes.byref(F), ctypes.c_int(nsteps),
+                    ctypes.c_double(Fconv), ctypes.c_int(conv_mode), ctypes.c_int(n_explore), ctypes.c_int(n_relax),
+                    ctypes.c_double(dt), ctypes.c_double(gamma), ctypes.c_double(T), ctypes.c_ulonglong(seed),
+                    ctypes.c_int(step0), ctypes.c_int(nthreads))
+    return dict(pos=pos, vel=vel, fire_state=fire_state, gopt=gopt, minpos=minpos)
+
+
 def surf(pos, REQ, sub, Rdamp=1.0):
     """Direct substrate term of atoms at pos [n,3] with REQ [n,4]: [n,4] (F, E)."""
     lib = orc()

@@ -151,6 +151,21 @@ int ref_relax(int niter, double Fconv, double* pos, double* vel, double* fire, d
     return itr;
 }
 
+// The exploring cycle of run_no_omp with bGopt (MolWorld_sp3.h:2290-2296,
+// 2397-2424, 2465-2473): GOpt on / off, its nExplore, the Langevin drive's
+// temperature and friction, and its current state (exploring, istep).  A
+// minimum found while relaxing makes run_no_omp append the geometry to
+// gopt.xyz in the working directory; the caller makes that open fail.
+void ref_set_gopt(int on, int nExplore, double T, double gamma, int exploring, int istep) {
+    W.bGopt = on != 0;
+    W.go.nExplore = nExplore;
+    W.go.T_target = T;
+    W.go.gamma_damp = gamma;
+    W.go.bExploring = exploring != 0;
+    W.go.istep = istep;
+}
+void ref_get_gopt(int* out) { out[0] = W.go.bExploring ? 1 : 0; out[1] = W.go.istep; }
+
 // Distance / angle constraints of the current system (after ref_setup), as
 // MolWorld_sp3::addDistConstrain (MolWorld_sp3.h:515-521) and libMMFF.h:45-47
 // add them; run_no_omp applies them when bConstrains is on.  dp rows: lmin,

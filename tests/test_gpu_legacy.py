@@ -113,3 +113,29 @@ def test_legacy_distance_and_angle_constraints(tmp_path, monkeypatch):
     assert np.isfinite(mmff.gpu_atoms).all()
     assert (held > free + 0.3).all(), (held, free)
     assert np.abs(held - held[0]).max() < 1e-3        # the same on every replica
+
+
+def test_legacy_run_explores_with_gopt(tmp_path, monkeypatch):
+    """init(T, gamma, nExplore, nRelax) + run(iParalel=2): the exploring cycle of
+    run_ocl_opt with GOpt; every replica starts exploring, the cycle's state
+    continues across calls and the replicas draw different noise."""
+    import ctypes
+    from firecore_b200 import MMFF_multi as mmff, _lib
+    monkeypatch.chdir(tmp_path)
+    mmff.init(nSys_=4, xyz_name=os.path.join(HERE, "mol24.xyz"), nPBC=(1, 1, 0), T=300.0, gamma=0.5, nExplore=20,
+              nRelax=150)
+    mmff.getBuffs()
+    p0 = mmff.gpu_atoms[:, :24, :3].copy()
+    assert mmff.run(nstepMax=300, Fconv=1e-3, iParalel=2) == 300
+    gopt = np.zeros((4, 4), np.int32)
+    lib = _lib.load()
+    assert lib.mmff_get_explore(ctypes.c_void_p(gopt.ctypes.data), None) == 0
+    assert (gopt[:, 2] + gopt[:, 3] >= 1).all(), gopt      # a phase ended on every replica
+    assert mmff.run(nstepMax=200, Fconv=1e-3, iParalel=2) == 200
+    g2 = np.zeros((4, 4), np.int32)
+    assert lib.mmff_get_explore(ctypes.c_void_p(g2.ctypes.data), None) == 0
+    assert (g2[:, 2] + g2[:, 3] >= gopt[:, 2] + gopt[:, 3]).all()
+    assert np.isfinite(mmff.gpu_atoms).all()
+    p = mmff.gpu_atoms[:, :24, :3]
+    assert np.abs(p - p0).max() > 1e-2
+    assert np.abs(p[1] - p[0]).max() > 1e-3                 # different noise per replica

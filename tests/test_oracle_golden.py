@@ -113,3 +113,68 @@ def test_constraints_match_reference_run_no_omp(golden):
     # and the constraints act: without them the trajectory differs
     r0 = O.relax(b, O.make_params(g, flags=flags), O.make_fire(), golden["C"], niter=nit, Fconv=1e-9, conv_mode=0)
     assert np.abs(r0["pos"] - pr).max() > 1e-3
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference harness not built (FireCore tree absent)")
+@pytest.mark.parametrize("fset", ["nogrid", "full"])
+def test_explore_cycle_matches_reference_run_no_omp(golden, fset, tmp_path, monkeypatch):
+    """The oracle's exploring cycle against FireCore's MolWorld_sp3::run_no_omp
+    with bGopt (GOpt update at the top of every step, FIRE scalars evolving while
+    exploring, a minimum starting an exploring phase), run live through the
+    reference harness: 1500 steps of one golden molecule that starts exploring,
+    with nExplore 15 and a noise-free drive (T = 0, friction 0.1).  run_no_omp
+    returns at every step where the system sits below Fconv, and its Langevin
+    step takes the FIRE dt of the call's start, so the oracle runs the same
+    pieces with that dt."""
+    import ctypes
+    # a minimum found makes run_no_omp append to ./gopt.xyz; a directory of
+    # that name makes the open fail before the write
+    monkeypatch.chdir(tmp_path)
+    (tmp_path / "gopt.xyz").mkdir()
+    b = batch_from_golden(golden, "A").subset([0])
+    g = grid_from_golden(golden)
+    flags = FLAGSETS[fset]
+    na, nn = int(b.natoms[0]), int(b.nnode[0])
+    ref = O.ref()
+    ref.ref_set_gopt.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int]
+    ref.ref_get_gopt.argtypes = [ctypes.c_void_p]
+    p = lambda a: ctypes.c_void_p(a.ctypes.data)  # noqa: E731
+    pos = np.ascontiguousarray(b.pos)
+    arr = [np.ascontiguousarray(x) for x in (b.neighs, b.neighCell, b.REQs)]
+    nar = [np.ascontiguousarray(x) for x in (b.apars, b.bLs, b.bKs, b.Ksp, b.Kpp)]
+    lv = np.ascontiguousarray(b.lvec[0].reshape(9))
+    npbc = np.array([1, 1, 0], np.int32)
+    gn = np.array(g.n, np.int32); gp0 = np.array(g.pos0); gst = np.array(g.step)
+    bk = np.zeros((na, 4), np.int32); ng = np.zeros((na, 4), np.int32)
+    C = np.ascontiguousarray(golden["C"])           # held: the harness reads it during the calls
+    ref.ref_setup(na, nn, p(pos), p(arr[0]), p(arr[1]), p(arr[2]), *[p(x) for x in nar], p(lv), p(npbc), flags, 1.5,
+                  p(gn), p(gp0), p(gst), p(C), p(bk), p(ng))
+    ref.ref_set_gopt(1, 15, 0.0, 0.1, 1, 0)
+    try:
+        pr = pos.copy(); vr = np.zeros_like(pr)
+        fr = np.array([0.1, 0.1, 0.0, 0.1, 0.01, 0.1, 1.1, 0.5, 0.8, 3, 0.0])
+        P = O.make_params(g, flags=flags); F = O.make_fire()
+        st = dict(pos=None, vel=None, fire_state=None, gopt=np.array([[1, 0, 0, 0]], np.int32), minpos=None)
+        total, found, N = 0, 0, 1500
+        gs = np.zeros(2, np.int32)
+        while total < N:
+            nit = N - total
+            oE = np.zeros(nit); oF = np.zeros(nit)
+            dt0 = fr[0]
+            it = ref.ref_relax(nit, 0.05, p(pr), p(vr), p(fr), p(oE), p(oF))
+            ref.ref_get_gopt(p(gs))
+            n = it + 1 if it < nit else nit          # run_no_omp breaks after step it
+            st = O.explore(b, P, F, golden["C"], nsteps=n, Fconv=0.05, conv_mode=0, n_explore=15,
+                           dt=float(np.float32(dt0)), gamma=0.1, T=0.0, pos=st["pos"], vel=st["vel"],
+                           fire_state=st["fire_state"], gopt=st["gopt"], minpos=st["minpos"])
+            assert tuple(st["gopt"][0][:2]) == tuple(gs)
+            assert np.abs(st["pos"] - pr).max() < 1e-9
+            assert np.abs(st["vel"] - vr).max() < 1e-9
+            assert np.abs(st["fire_state"][0, :3] - fr[:3]).max() < 1e-9
+            if gs[0] == 1 and gs[1] == 0:            # a minimum ended this call
+                found += 1
+                assert np.abs(st["minpos"] - pr).max() < 1e-9
+            total += n
+        assert found >= 3 and int(st["gopt"][0][2]) == found
+    finally:
+        ref.ref_set_gopt(0, 0, 0.0, 0.0, 0, 0)
