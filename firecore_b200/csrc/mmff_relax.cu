@@ -1140,8 +1140,9 @@ template <int T> constexpr int relax_min_blocks() {
 }
 
 // P.vlist (null: none): scratch for the shifted-image pair lists, P.vstride
-// 32-bit words per CTA (P.vcap entries, then 4 * maxNA words of positions)
-template <int T, int S, bool COUNT>
+// 32-bit words per CTA (P.vcap entries, then 4 * maxNA words of positions).
+// EXPL: the exploring cycle (P.md_mode 2) instead of plain FIRE or the drive.
+template <int T, int S, bool COUNT, bool EXPL = false>
 __global__ void __launch_bounds__(T, relax_min_blocks<T>()) relax_kernel(Params P, Systems Y, const int* __restrict__ queue, int nqueue,
                                                   int* counter, int maxNA, int maxNN) {
     extern __shared__ __align__(16) char smem[];
@@ -1163,12 +1164,12 @@ __global__ void __launch_bounds__(T, relax_min_blocks<T>()) relax_kernel(Params 
         int status = ST_MAXSTEPS, itr = 0;
         float meas = 0.f;
         int ph = 0;                 // exploring cycle: 2 * (steps in the phase) + exploring
-        if (P.md_mode == 2) { const int4 g = Y.gopt[s]; ph = 2 * g.y + (g.x != 0); }
+        if constexpr (EXPL) { const int4 g = Y.gopt[s]; ph = 2 * g.y + (g.x != 0); }
         for (itr = 0; itr < P.nstep_max; itr++) {
-            bool expl = false;
-            if (P.md_mode == 2) {
+            bool lang = false;      // an exploring step (Langevin instead of FIRE)
+            if constexpr (EXPL) {
                 const int ev = explore_step(ph, P.n_explore, P.n_relax);
-                expl = ev & 1;
+                lang = ev & 1;
                 if ((ev & 2) && threadIdx.x == 0) Y.gopt[s].w++;
             }
             double d0 = 0, d1 = 0, d2 = 0;
@@ -1180,7 +1181,7 @@ __global__ void __launch_bounds__(T, relax_min_blocks<T>()) relax_kernel(Params 
             E.assemble(vf, vv, ff, fmax2, bad);
             E.reduce4(vf, vv, ff, fmax2, bad);
             if (bad) { status = ST_NAN; break; }
-            if (P.md_mode == 1) {   // Langevin drive: fixed number of steps, no FIRE
+            if (!EXPL && P.md_mode) {   // Langevin drive: fixed number of steps, no FIRE
                 float mn[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, mx[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
                 E.move_md(P.md_step0 + itr, mn, mx);
                 total += 1.0;
@@ -1188,7 +1189,9 @@ __global__ void __launch_bounds__(T, relax_min_blocks<T>()) relax_kernel(Params 
                 E.bbox_reduce(mn, mx);
                 continue;
             }
-            // DynamicOpt::FIRE_update_params (FP64, identical in every thread)
+            // DynamicOpt::FIRE_update_params (FP64, identical in every thread); in the
+            // exploring cycle the FIRE scalars evolve in exploring steps too
+            // (MolWorld_sp3.h:2401-2424)
             const double f_len = sqrt(ff), v_len = sqrt(vv);
             const double cos_vf = vf / (f_len * v_len + 1e-32);
             const double renorm_vf = v_len / (f_len + 1e-32);
@@ -1204,18 +1207,20 @@ __global__ void __launch_bounds__(T, relax_min_blocks<T>()) relax_kernel(Params 
                 lastNeg++;
             }
             float mn[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, mx[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
-            // the FIRE scalars above evolve in exploring steps too (MolWorld_sp3.h:2401-2424)
-            if (expl) E.move_md(P.md_step0 + itr, mn, mx);
+            if (EXPL && lang) E.move_md(P.md_step0 + itr, mn, mx);
             else E.move(dt, cv, P.fire_variant == 1 ? cf : renorm_vf * cf, mn, mx);
             total += 1.0;
             const double m = (P.conv_mode == 0) ? ff : (double)fmax2;
             meas = (float)sqrt(m);
-            if (m < P.Fconv2 && !expl) {
-                if (P.md_mode != 2) { status = ST_CONVERGED; itr++; E.bbox_reduce(mn, mx); break; }
-                // a minimum (MolWorld_sp3.h:2465-2473): keep it, start exploring
-                E.snapshot();
-                if (threadIdx.x == 0) Y.gopt[s].z++;
-                ph = 1;
+            if constexpr (EXPL) {
+                if (!lang && m < P.Fconv2) {
+                    // a minimum (MolWorld_sp3.h:2465-2473): keep it, start exploring
+                    E.snapshot();
+                    if (threadIdx.x == 0) Y.gopt[s].z++;
+                    ph = 1;
+                }
+            } else {
+                if (m < P.Fconv2) { status = ST_CONVERGED; itr++; E.bbox_reduce(mn, mx); break; }
             }
             E.bbox_reduce(mn, mx);   // contains the end-of-step barrier
         }
@@ -1223,7 +1228,7 @@ __global__ void __launch_bounds__(T, relax_min_blocks<T>()) relax_kernel(Params 
         const int steps = (status == ST_CONVERGED) ? itr - 1 : itr;
         __syncthreads();
         E.store_state(status, steps, meas, dt, damping, lastNeg, total);
-        if (P.md_mode == 2 && threadIdx.x == 0) { Y.gopt[s].x = ph & 1; Y.gopt[s].y = ph >> 1; }
+        if (EXPL && threadIdx.x == 0) { Y.gopt[s].x = ph & 1; Y.gopt[s].y = ph >> 1; }
         if (COUNT) {
             // force evaluations done for this system: itr loop iterations
             if (threadIdx.x == 0) {
@@ -1323,6 +1328,16 @@ __global__ void grid_sample_kernel(Params P, int n, const float4* __restrict__ p
 void* relax_fn(int T, int S, bool count) {
     if (count) { MMFF_TS_SWITCH(T, S, return (void*)relax_kernel<T_, S_, true>) }
     MMFF_TS_SWITCH(T, S, return (void*)relax_kernel<T_, S_, false>)
+}
+// the exploring cycle runs one pair lane per atom (S = 1) at any block size
+void* relax_explore_fn(int T) {
+    switch (T) {
+        case 64: return (void*)relax_kernel<64, 1, false, true>;
+        case 128: return (void*)relax_kernel<128, 1, false, true>;
+        case 256: return (void*)relax_kernel<256, 1, false, true>;
+        case 512: return (void*)relax_kernel<512, 1, false, true>;
+        default: return nullptr;
+    }
 }
 void* eval_fn(int T, int S, bool energy) {
     if (energy) { MMFF_TS_SWITCH(T, S, return (void*)eval_kernel<T_, S_, true>) }

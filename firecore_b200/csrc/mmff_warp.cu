@@ -684,7 +684,8 @@ struct WarpEngine {
 #ifndef MMFF_WARP_MINB
 #define MMFF_WARP_MINB 4
 #endif
-template <int APL, bool COUNT>
+// EXPL: the exploring cycle (P.md_mode 2) instead of plain FIRE or the drive.
+template <int APL, bool COUNT, bool EXPL = false>
 __global__ void __launch_bounds__(128, MMFF_WARP_MINB) relax_warp_kernel(Params P, Systems Y, const int* __restrict__ queue, int nqueue,
                                                          int* counter, int maxNA, int maxNN) {
     extern __shared__ __align__(16) char smem[];
@@ -705,12 +706,12 @@ __global__ void __launch_bounds__(128, MMFF_WARP_MINB) relax_warp_kernel(Params 
         int status = ST_MAXSTEPS, itr = 0;
         float meas = 0.f;
         int ph = 0;                 // exploring cycle: 2 * (steps in the phase) + exploring
-        if (P.md_mode == 2) { const int4 g = Y.gopt[s]; ph = 2 * g.y + (g.x != 0); }
+        if constexpr (EXPL) { const int4 g = Y.gopt[s]; ph = 2 * g.y + (g.x != 0); }
         for (itr = 0; itr < P.nstep_max; itr++) {
-            bool expl = false;
-            if (P.md_mode == 2) {
+            bool lang = false;      // an exploring step (Langevin instead of FIRE)
+            if constexpr (EXPL) {
                 const int ev = explore_step(ph, P.n_explore, P.n_relax);
-                expl = ev & 1;
+                lang = ev & 1;
                 if ((ev & 2) && lane == 0) Y.gopt[s].w++;
             }
             double d0 = 0, d1 = 0, d2 = 0;
@@ -720,13 +721,15 @@ __global__ void __launch_bounds__(128, MMFF_WARP_MINB) relax_warp_kernel(Params 
             bool bad;
             E.fire_sums(vf, vv, ff, fmax2, bad);
             if (bad) { status = ST_NAN; break; }
-            if (P.md_mode == 1) {   // Langevin drive: fixed number of steps, no FIRE
+            if (!EXPL && P.md_mode) {   // Langevin drive: fixed number of steps, no FIRE
                 E.move_md(P.md_step0 + itr);
                 total += 1.0;
                 meas = sqrtf(fmax2);
                 continue;
             }
-            // DynamicOpt::FIRE_update_params (DynamicOpt.cpp:250-267), FP64
+            // DynamicOpt::FIRE_update_params (DynamicOpt.cpp:250-267), FP64; in the
+            // exploring cycle the FIRE scalars evolve in exploring steps too
+            // (MolWorld_sp3.h:2401-2424)
             const double f_len = sqrt(ff), v_len = sqrt(vv);
             const double cos_vf = vf / (f_len * v_len + 1e-32);
             const double renorm_vf = v_len / (f_len + 1e-32);
@@ -741,23 +744,25 @@ __global__ void __launch_bounds__(128, MMFF_WARP_MINB) relax_warp_kernel(Params 
                 if (lastNeg > P.minLastNeg) { dt = fmin(dt * P.finc, P.dt_max); damping = damping * P.falpha; }
                 lastNeg++;
             }
-            // the FIRE scalars above evolve in exploring steps too (MolWorld_sp3.h:2401-2424)
-            if (expl) E.move_md(P.md_step0 + itr);
+            if (EXPL && lang) E.move_md(P.md_step0 + itr);
             else E.move(dt, cv, P.fire_variant == 1 ? cf : renorm_vf * cf);
             total += 1.0;
             const double m = (P.conv_mode == 0) ? ff : (double)fmax2;
             meas = (float)sqrt(m);
-            if (m < P.Fconv2 && !expl) {
-                if (P.md_mode != 2) { status = ST_CONVERGED; itr++; break; }
-                // a minimum (MolWorld_sp3.h:2465-2473): keep it, start exploring
-                E.snapshot();
-                if (lane == 0) Y.gopt[s].z++;
-                ph = 1;
+            if constexpr (EXPL) {
+                if (!lang && m < P.Fconv2) {
+                    // a minimum (MolWorld_sp3.h:2465-2473): keep it, start exploring
+                    E.snapshot();
+                    if (lane == 0) Y.gopt[s].z++;
+                    ph = 1;
+                }
+            } else {
+                if (m < P.Fconv2) { status = ST_CONVERGED; itr++; break; }
             }
         }
         const int steps = (status == ST_CONVERGED) ? itr - 1 : itr;
         E.store(status, steps, meas, dt, damping, lastNeg, total);
-        if (P.md_mode == 2 && lane == 0) { Y.gopt[s].x = ph & 1; Y.gopt[s].y = ph >> 1; }
+        if (EXPL && lane == 0) { Y.gopt[s].x = ph & 1; Y.gopt[s].y = ph >> 1; }
         if (COUNT && lane == 0) {
             atomicAdd(Y.counters + 1, (unsigned long long)itr * (unsigned long long)E.N);
             atomicAdd(Y.counters + 2, (unsigned long long)itr);
@@ -809,6 +814,11 @@ __global__ void __launch_bounds__(128) eval_warp_kernel(Params P, Systems Y, con
 void* relax_warp_fn(int apl, bool count) {
     if (apl == 1) return count ? (void*)relax_warp_kernel<1, true> : (void*)relax_warp_kernel<1, false>;
     if (apl == 2) return count ? (void*)relax_warp_kernel<2, true> : (void*)relax_warp_kernel<2, false>;
+    return nullptr;
+}
+void* relax_warp_explore_fn(int apl) {
+    if (apl == 1) return (void*)relax_warp_kernel<1, false, true>;
+    if (apl == 2) return (void*)relax_warp_kernel<2, false, true>;
     return nullptr;
 }
 void* eval_warp_fn(int apl, bool energy) {

@@ -34,6 +34,8 @@ __global__ void pack_grid_kernel(long, const double*, float4*);
 void* relax_fn(int T, int S, bool count);
 void* eval_fn(int T, int S, bool energy);
 void* relax_warp_fn(int apl, bool count);
+void* relax_explore_fn(int T);
+void* relax_warp_explore_fn(int apl);
 void* eval_warp_fn(int apl, bool energy);
 
 }  // namespace mmff
@@ -294,6 +296,9 @@ int config_bucket(Bucket& B, int kind, int apl, int T, int S) {
     if (B.smem > dev_smem) return fail("system too large for shared memory: %d B > %d B", B.smem, dev_smem);
     if (!fns[0] || !fns[1]) return fail("no kernel for bucket (kind %d, T=%d, S=%d)", B.kind, B.T, B.S);
     for (int f = 0; f < 2; f++) if (set_smem_limit(fns[f], B.smem)) return -1;
+    void* xf = B.kind ? relax_warp_explore_fn(B.apl) : relax_explore_fn(B.T);     // exploring cycle
+    if (!xf) return fail("no exploring-cycle kernel for bucket (kind %d, T=%d)", B.kind, B.T);
+    if (set_smem_limit(xf, B.smem)) return -1;
     for (int e = 0; e < 2; e++) {
         void* ef = B.kind ? eval_warp_fn(B.apl, e) : eval_fn(B.T, B.S, e);
         if (set_smem_limit(ef, B.smem)) return -1;
@@ -484,7 +489,8 @@ int enqueue_relax(const Params& P) {
         Bucket& B = W.buckets[b];
         cudaStream_t st = W.bstreams[b];
         CK(cudaStreamWaitEvent(st, W.evfork, 0));
-        void* fn = B.kind ? relax_warp_fn(B.apl, W.count) : relax_fn(B.T, B.S, W.count);
+        void* fn = P.md_mode == 2 ? (B.kind ? relax_warp_explore_fn(B.apl) : relax_explore_fn(B.T))
+                                  : (B.kind ? relax_warp_fn(B.apl, W.count) : relax_fn(B.T, B.S, W.count));
         const int* q = B.queue.p;
         int nq = (int)B.sys.size();
         int* ctr = W.d_counter.p + b;
