@@ -89,3 +89,35 @@ def test_c0_relaxed_replicas(c0):
     tight = [float(np.sqrt(((td["pos"][vb[k]:vb[k] + sb.natoms[k]] - to["pos"][vb[k]:vb[k] + sb.natoms[k]]) ** 2)
                            .sum(1).mean())) for k in range(sb.nsys)]
     assert max(tight) <= 1e-3, tight
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference harness not built (FireCore tree absent)")
+def test_c0_oracle_matches_firecore_run_no_omp(c0):
+    """On this configuration the checker itself agrees with FireCore's own
+    MolWorld_sp3::run_no_omp (compiled from its sources into the harness) on
+    the GPU-built grid: every replica's step count and end point."""
+    import ctypes
+    w, b, sub, C = c0
+    g = sub.grid
+    ref = O.ref()
+    p = lambda a: ctypes.c_void_p(a.ctypes.data)  # noqa: E731
+    a_off, n_off, v_off = b.offsets()
+    npbc = np.array([1, 1, 0], np.int32)
+    gn = np.array(g.n, np.int32); gp0 = np.array(g.pos0); gst = np.array(g.step)
+    Cc = np.ascontiguousarray(C)            # held: the harness reads it during the calls
+    r = O.relax(b, O.make_params(g, npbc=(1, 1, 0)), O.make_fire(), C, niter=NSTEP, Fconv=FCONV, conv_mode=0)
+    for s in range(b.nsys):
+        na, nn = int(b.natoms[s]), int(b.nnode[s])
+        pos = np.ascontiguousarray(b.pos[v_off[s]:v_off[s + 1]])
+        arr = [np.ascontiguousarray(x[a_off[s]:a_off[s + 1]]) for x in (b.neighs, b.neighCell, b.REQs)]
+        nar = [np.ascontiguousarray(x[n_off[s]:n_off[s + 1]]) for x in (b.apars, b.bLs, b.bKs, b.Ksp, b.Kpp)]
+        lv = np.ascontiguousarray(b.lvec[s].reshape(9))
+        bk = np.zeros((na, 4), np.int32); ng = np.zeros((na, 4), np.int32)
+        ref.ref_setup(na, nn, p(pos), p(arr[0]), p(arr[1]), p(arr[2]), *[p(x) for x in nar], p(lv), p(npbc),
+                      O.DEFAULT_FLAGS, 1.5, p(gn), p(gp0), p(gst), p(Cc), p(bk), p(ng))
+        vel = np.zeros_like(pos)
+        fire = np.array([0.1, 0.1, 0.0, 0.1, 0.01, 0.1, 1.1, 0.5, 0.8, 3, 0.0])
+        oE = np.zeros(NSTEP); oF = np.zeros(NSTEP)
+        it = ref.ref_relax(NSTEP, FCONV, p(pos), p(vel), p(fire), p(oE), p(oF))
+        assert it == int(r["nsteps"][s]), (s, it, r["nsteps"][s])
+        assert np.abs(pos - r["pos"][v_off[s]:v_off[s + 1]]).max() < 1e-8, s
