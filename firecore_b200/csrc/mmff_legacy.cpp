@@ -248,6 +248,7 @@ struct LegacyWorld {
     bool md_set = false;          // Langevin parameters passed to the device world
     // exploring cycle of init(nExplore, nRelax) (GOpt): run(iParalel = 2) drives it
     int nExplore = 0, nRelax = 0;
+    int explore_nrelax = -1;      // the give-up rule the device cycle was set up with
     // host mirrors (pyBall/MMFF_multi.py:238-256 shapes)
     std::vector<float> atoms, aforces, avel, constr, REQs, MMpars, BLs, BKs, Ksp, Kpp, lvecs, ilvecs, pbcshifts;
     // spring constants of the constr anchors (MolWorld_sp3_multi::constrK): -1 = no
@@ -441,7 +442,7 @@ void* init(int nSys, char* xyz_name, char* surf_name, char* smile_name, bool bMM
     // pos_kick / vel_kick feed GOpt::apply_kick, which the reference never calls
     (void)smile_name; (void)bMMFF; (void)pos_kick; (void)vel_kick;
     L.T = T; L.gamma = gamma; L.md_set = false;
-    L.nExplore = nExplore; L.nRelax = nRelax;
+    L.nExplore = nExplore; L.nRelax = nRelax; L.explore_nrelax = -1;
     L.dist_i.clear(); L.dist_p.clear(); L.ang_i.clear(); L.ang_p.clear();
     {   // a new world: the cell of an earlier init (its substrate or xyz) does not carry over
         const double lv0[9] = {20, 0, 0, 0, 20, 0, 0, 0, 20};
@@ -556,17 +557,22 @@ void* init(int nSys, char* xyz_name, char* surf_name, char* smile_name, bool bMM
 int run(int nstepMax, double dt, double Fconv, int ialg, double* outE, double* outF, int iParalel) {
     (void)dt; (void)ialg;
     if (!L.ready) { set_error("run: init() first"); return -1; }
-    if (iParalel == 2 && L.nExplore > 0) {
-        // run_ocl_opt with GOpt (MolWorld_sp3_multi.h:1694-1846, 770-833): every
-        // replica cycles between FIRE and nExplore Langevin steps (time step =
-        // the FIRE dt_max, as evalVF_new sets it, MolWorld_sp3_multi.h:756-760);
-        // after init every replica starts exploring (MolWorld_sp3_multi.h:278).
-        // The cycle's state lives on the device until the systems are uploaded again.
-        if (mmff_get_explore(nullptr, nullptr)) {
-            if (mmff_set_md(L.fire[0], L.gamma, L.T, 12345ull) || mmff_set_explore(L.nExplore, L.nRelax, 1)) {
+    if (iParalel >= 0 && iParalel <= 2 && L.nExplore > 0) {
+        // run_omp_ocl (iParalel 0, 1) and run_ocl_opt (2) with GOpt, which init
+        // switches on (MMFFmulti_lib.cpp:88; MolWorld_sp3_multi.h:1970-2050,
+        // 1694-1846, 770-833): every replica cycles between FIRE and nExplore
+        // Langevin steps (time step = the FIRE dt_max, MolWorld_sp3_multi.h:756-760,
+        // 2012); only run_ocl_opt gives up a relax phase after nRelax steps.
+        // After init every replica starts exploring (MolWorld_sp3_multi.h:278).
+        // The cycle's state lives on the device until the systems are uploaded
+        // again or the give-up rule changes.
+        const int nrelax = iParalel == 2 ? L.nRelax : 0;
+        if (mmff_get_explore(nullptr, nullptr) || nrelax != L.explore_nrelax) {
+            if (mmff_set_md(L.fire[0], L.gamma, L.T, 12345ull) || mmff_set_explore(L.nExplore, nrelax, 1)) {
                 set_error(mmff_last_error()); return -1;
             }
             L.md_set = true;
+            L.explore_nrelax = nrelax;
         }
         if (mmff_explore(nstepMax, Fconv, 0)) { set_error(mmff_last_error()); return -1; }
     } else if (mmff_relax(nstepMax, Fconv, 0)) { set_error(mmff_last_error()); return -1; }
@@ -583,10 +589,18 @@ int run(int nstepMax, double dt, double Fconv, int ialg, double* outE, double* o
     return mx;
 }
 
-// MolWorld_sp3_multi::MDloop: FIRE relaxation, or with init(T > 0, gamma > 0)
-// perframe steps of the Langevin drive (time step = the FIRE dt_max)
+// MolWorld_sp3_multi::MDloop: perframe steps of the path its iParalel selects
+// (MolWorld_sp3_multi.h:2236-2243: 0 run_no_omp, 1-2 run_omp_ocl, 3 run_ocl_opt),
+// i.e. FIRE relaxation, or with init's nExplore > 0 the exploring cycle; with
+// nExplore = 0 and init(T > 0, gamma > 0) the Langevin drive for every replica
+// instead (time step = the FIRE dt_max), which FireCore only applies to
+// exploring replicas
 void MDloop(int perframe, double Ftol, int iParalel, int perVF) {
     (void)perVF;
+    if (L.ready && L.nExplore > 0 && iParalel >= 0 && iParalel <= 3) {
+        run(perframe, -1, Ftol > 0 ? Ftol : 1e-6, 0, nullptr, nullptr, iParalel == 3 ? 2 : 1);
+        return;
+    }
     if (L.ready && L.T > 0 && L.gamma > 0) {
         if (!L.md_set && mmff_set_md(L.fire[0], L.gamma, L.T, 12345ull)) { set_error(mmff_last_error()); return; }
         L.md_set = true;

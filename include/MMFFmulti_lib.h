@@ -312,10 +312,12 @@ void* init(int nSys, char* xyz_name, char* surf_name, char* smile_name, bool bMM
  * pos_kick and vel_kick (the reference's GOpt::apply_kick is never called). */
 int   run(int nstepMax, double dt, double Fconv, int ialg, double* outE, double* outF, int iParalel);   /* :116 */
 /* run: FIRE relaxation of every replica for up to nstepMax steps (every
- * iParalel); with iParalel = 2 and init's nExplore > 0, nstepMax steps of the
- * exploring cycle instead (mmff_explore; Langevin time step = the FIRE dt_max,
- * T and gamma from init, every replica starting in an exploring phase), as
- * run_ocl_opt with GOpt does.  dt and ialg are ignored, as by the reference. */
+ * iParalel); with init's nExplore > 0 and iParalel 0, 1 or 2, nstepMax steps
+ * of the exploring cycle instead (mmff_explore; Langevin time step = the FIRE
+ * dt_max, T and gamma from init, every replica starting in an exploring
+ * phase), as run_omp_ocl and run_ocl_opt with GOpt do; only iParalel 2 gives
+ * up a relax phase after nRelax steps (run_ocl_opt's rule).  dt and ialg are
+ * ignored, as by the reference. */
 void  MDloop(int perframe, double Ftol, int iParalel, int perVF);           /* :134 */
 void  set_opt(double dt_max, double dt_min, double damp_max, double finc, double fdec, double falpha, int minLastNeg,
               double cvf_min, double cvf_max);                              /* :141 */

@@ -135,6 +135,10 @@ def test_legacy_run_explores_with_gopt(tmp_path, monkeypatch):
     g2 = np.zeros((4, 4), np.int32)
     assert lib.mmff_get_explore(ctypes.c_void_p(g2.ctypes.data), None) == 0
     assert (g2[:, 2] + g2[:, 3] >= gopt[:, 2] + gopt[:, 3]).all()
+    mmff.MDloop(perframe=100, iParalel=3)                  # MDloop's run_ocl_opt: the same cycle goes on
+    g3 = np.zeros((4, 4), np.int32)
+    assert lib.mmff_get_explore(ctypes.c_void_p(g3.ctypes.data), None) == 0
+    assert (g3[:, 2] + g3[:, 3] >= g2[:, 2] + g2[:, 3]).all()
     assert np.isfinite(mmff.gpu_atoms).all()
     p = mmff.gpu_atoms[:, :24, :3]
     assert np.abs(p - p0).max() > 1e-2
