@@ -99,8 +99,14 @@ def test_explore_needs_setup(world):
     world.upload(b)
     with pytest.raises(RuntimeError, match="mmff_set_explore"):
         world.explore(5)
+    with pytest.raises(RuntimeError, match="no exploring cycle"):
+        world.explore_state()
+    with pytest.raises(RuntimeError, match="n_explore must be >= 0"):
+        world.set_explore(-1, 0)
     world.set_explore(4, 0)
     world.explore(5)
+    gopt, _ = world.explore_state()
+    assert (gopt[:, 1] >= 0).all() and gopt.shape == (2, 4)
     world.upload(b)                       # new systems: the cycle is set up again
     with pytest.raises(RuntimeError, match="mmff_set_explore"):
         world.explore(5)
